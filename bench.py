@@ -1,0 +1,372 @@
+"""Benchmark of the mine.cu environment step on B200.
+
+Workload (the headline "peak shape"): B=32768 envs per GPU, world 16^3,
+32x32 RGB uint8 observations (obs_dtype "uint8", the shaded kernels),
+max_steps 64, view distance 32, fov 70, target block OAKLOG, no episode
+limit; synthetic discrete actions uniform over the 11 actions from a seeded
+Philox4x32-10 stream (seed 1; counter = (global env, step)).
+
+Metric: env-steps/s (B x steps x GPUs / time), higher is better.
+  value  the fused step (one persistent kernel per step) of K steps captured
+         in a CUDA graph, actions resident in HBM, timed with CUDA events on
+         the launching stream, max over ranks.
+  e2e    MineEnv.step(actions) through the public API, every step copying
+         that step's actions from pinned host memory and the step's rewards
+         and dones back to pinned host memory (asynchronously, read after the
+         timed loop).
+  plain  the reference's kernel sequence (one kernel per reference kernel).
+The per-step working set (worlds 134 MB + observations 101 MB) exceeds the
+126 MB L2, so no flush is done between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W]
+  python bench.py --impl reference   # the reference's own CUDA build, same workload
+
+With --gpus N > 1 launch one process per GPU with torch.distributed.run;
+each rank steps its own B envs (weak scaling, no collective in the step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mine.cu_b200"))
+
+WORKLOAD = dict(workload="peak shape: B=32768 envs/GPU, world 16^3, 32x32x3 uint8 obs (shaded), "
+                "uniform discrete actions seed 1", batch_size=32768, world=16, res=32, obs_dtype="uint8",
+                max_steps=64, seed=1, look_delta=0.1)
+BYTES_PER_ENV_STEP = 16 ** 3 + 32 * 32 * 3  # world read + obs written (algorithmic)
+METRIC = "env-steps/s at B=32K, W=16, 32x32 (fused step, CUDA graph)"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i, v in enumerate(s[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    if n_gpus > 1 or "RANK" in os.environ:
+        rank = int(os.environ.get("RANK", 0))
+        world = int(os.environ.get("WORLD_SIZE", 1))
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        torch.cuda.set_device(local)
+        if world > 1:
+            import datetime
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        return rank, world, local
+    torch.cuda.set_device(0)
+    return 0, 1, 0
+
+
+def barrier(world):
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(seconds=12.0, B=2048):
+    """The CPU restatement of the step (oracle/mc_oracle.c, IEEE numerics,
+    OpenMP over envs) on this host's cores, on a bounded sample: B envs of
+    the same workload stepped until `seconds` have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    W = WORKLOAD
+    e = O.OracleEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                    obs_dtype=W["obs_dtype"], max_steps=W["max_steps"], threads=cores)
+    e.reset()
+    acts = [O.discrete_to_buttons(O.philox_actions(B, s, W["seed"]), W["look_delta"]) for s in range(64)]
+    for s in range(3):  # warm-up
+        e.step(*acts[s])
+    n, t0 = 0, time.perf_counter()
+    while True:
+        e.step(*acts[(n + 3) % 64])
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 500:
+            break
+    return {"value": B * n / el, "unit": "env-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{B} envs x {n} steps of the same workload ({el:.1f} s), oracle/mc_oracle.c with "
+                      f"{cores} OpenMP threads"}
+
+
+def run_mine(args):
+    import torch
+    from minecu import MineEnv, _C
+
+    rank, world, local = dist_setup(args.gpus)
+    W = WORKLOAD
+    B, K, Wm = W["batch_size"], args.steps, args.warmup
+    dev = torch.device("cuda", local)
+    env = MineEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                  device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], numerics="ref_fast",
+                  form="fused", look_delta=W["look_delta"])
+    if args.launch:
+        st, wpc, cps, ppl = (int(x) for x in args.launch.split(","))
+        env.set_launch_config(st, wpc, cps, ppl)
+    env.reset()
+    stream = torch.cuda.current_stream()
+    acts_w = torch.empty((max(Wm, 1), B), dtype=torch.uint8, device=dev)
+    acts_t = torch.empty((K, B), dtype=torch.uint8, device=dev)
+    _C.philox_actions(acts_w, rank * B, 0, W["seed"])
+    _C.philox_actions(acts_t, rank * B, Wm, W["seed"])
+    env.prepare_rollout(acts_w)
+    env.prepare_rollout(acts_t)
+    torch.cuda.synchronize()
+
+    # ---- fused step in a CUDA graph (value) --------------------------------
+    env.rollout(acts_w[:Wm] if Wm else acts_w[:0])
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        env.rollout(acts_t)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t_fused = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    env.check_error()
+    value = B * K * world / t_fused
+    ms_step = t_fused / K * 1e3
+
+    # ---- plain form (the reference's kernel sequence, eager) ---------------
+    Kp = min(K, args.plain_steps)
+    env.form = "plain"
+    for s in range(min(Wm, 5)):
+        env.step(acts_w[s % acts_w.shape[0]])
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0.record(stream)
+    for s in range(Kp):
+        env.step(acts_t[s])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    plain_value = B * Kp * world / t_plain
+    env.form = "fused"
+
+    # ---- e2e through the public API with host buffers ------------------------
+    Ke = min(K, args.e2e_steps)
+    h_acts = acts_t[:Ke].cpu().pin_memory()
+    h_rew = torch.empty((Ke, B), dtype=torch.float32).pin_memory()
+    h_done = torch.empty((Ke, B), dtype=torch.bool).pin_memory()
+    d_act = torch.empty((B,), dtype=torch.uint8, device=dev)
+    for s in range(min(Wm, 5)):
+        d_act.copy_(h_acts[s], non_blocking=True)
+        env.step(d_act)
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0.record(stream)
+    for s in range(Ke):
+        d_act.copy_(h_acts[s], non_blocking=True)
+        obs, rew, done = env.step(d_act)
+        h_rew[s].copy_(rew, non_blocking=True)
+        h_done[s].copy_(done, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    e2e_value = B * Ke * world / t_e2e
+    _ = float(h_rew.sum())  # the host reads the results
+
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_ENV_STEP * B / (t_fused / K) / 1e9
+    traffic = None
+    if args.traffic_bytes:
+        traffic = float(args.traffic_bytes)
+    line = {
+        "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
+        "config": {"workload": W["workload"], "global_batch": B * world, "world": "16x16x16",
+                   "render": "32x32x3 uint8", "obs_dtype": W["obs_dtype"], "numerics": "ref_fast",
+                   "form": "fused persistent kernel, K-step CUDA graph", "launch": env.launch_config(),
+                   "parallelism": f"env-sharded x{world} (no collective)",
+                   "l2": "per-step working set 235 MB (worlds 134 MB + obs 101 MB) > 126 MB L2; no flush"},
+        "plain": {"value": plain_value, "unit": "env-steps/s", "steps": Kp,
+                  "ms_per_step": t_plain / Kp * 1e3, "fused_speedup": value / plain_value},
+        "e2e": {"value": e2e_value, "unit": "env-steps/s", "steps": Ke, "h2d_bytes_per_step": B,
+                "d2h_bytes_per_step": B * 4 + B,
+                "path": "MineEnv.step(actions) per step; pinned H2D actions, D2H rewards+dones"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_env_step": BYTES_PER_ENV_STEP,
+                     "kernel": "k_step_fused (avg over the timed region)"},
+        "gpu_launches": K,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own CUDA build (oracle/_ref/libminecu_ref.so, its
+    src/kernels.cu compiled unmodified) driven in its MineEnv.step order, on
+    the same workload.  The reference has no CPU implementation; its stock
+    implementation of this path is these kernels."""
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import ref_driver
+    W = WORKLOAD
+    if not ref_driver.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libminecu_ref.so not built"}))
+        return
+    B, K, Wm = W["batch_size"], args.steps, args.warmup
+    dev = torch.device("cuda", local)
+    env = ref_driver.RefEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                            device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], target_block=3)
+    env.reset()
+    Kr = min(K, args.ref_steps)
+    btns = torch.empty((Kr + Wm, B, 8), dtype=torch.int8)
+    looks = torch.empty((Kr + Wm, B, 2), dtype=torch.float32)
+    for s in range(Kr + Wm):
+        b, l = O.discrete_to_buttons(O.philox_actions(B, s, W["seed"]), W["look_delta"])
+        btns[s] = torch.from_numpy(b)
+        looks[s] = torch.from_numpy(l)
+    d_btn, d_look = btns.to(dev), looks.to(dev)
+    for s in range(Wm):
+        env.step(d_btn[s], d_look[s])
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(Kr):
+        env.step(d_btn[Wm + s], d_look[Wm + s])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3
+    value = B * Kr / t
+    # e2e: actions from pinned host memory, rewards + dones back, every step
+    h_btn, h_look = btns.pin_memory(), looks.pin_memory()
+    h_rew = torch.empty((Kr, B), dtype=torch.float32).pin_memory()
+    h_done = torch.empty((Kr, B), dtype=torch.bool).pin_memory()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in range(Kr):
+        obs, rew, done = env.step(h_btn[Wm + s].to(dev, non_blocking=True), h_look[Wm + s].to(dev, non_blocking=True))
+        h_rew[s].copy_(rew, non_blocking=True)
+        h_done[s].copy_(done, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    te = ev0.elapsed_time(ev1) / 1e3
+    e2e = B * Kr / te
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": 1, "steps": Kr,
+        "warmup": Wm, "ms_per_step": t / Kr * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
+        "config": {"workload": W["workload"], "global_batch": B, "obs_dtype": W["obs_dtype"],
+                   "path": "reference src/kernels.cu launch_step_uint8 + MineEnv.step glue (eager, default stream)"},
+        "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": B * 16, "d2h_bytes_per_step": B * 5},
+        "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": None, "kind": "reference",
+                         "sample": f"{Kr} steps of B={B}; the reference implementation is CUDA-only, so this arm "
+                                   "runs its own kernels on the same B200"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=200)
+    ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--ref-steps", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,px_per_lane")
+    ap.add_argument("--traffic-bytes", type=float, default=0.0,
+                    help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mine(args)
+
+
+if __name__ == "__main__":
+    main()

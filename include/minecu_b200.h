@@ -1,0 +1,232 @@
+/*
+ * minecu_b200.h - C-ABI of libminecu_b200.so, the B200 implementation of
+ * mine.cu's environment step.
+ *
+ * The reference exposes its step as `extern "C"` launchers in
+ * src/kernels.cu:2076-3245 (launch_step*, launch_render*, launch_generate_world,
+ * ...) bound by pybind11 in src/bindings.cpp.  Those take raw device
+ * pointers, run on the legacy default stream, return void and keep
+ * process-global CUDA-graph state.  The entry points below take the same
+ * pointers and sizes, plus an explicit CUDA stream (`void*` holding a
+ * cudaStream_t, NULL = legacy default stream) and return an int status
+ * (MC_OK or a negative MC_ERR_*; mc_last_error() gives the message).
+ *
+ * Ownership: the caller owns every state buffer (as the reference's
+ * MineEnv owns its torch tensors, minecu/__init__.py:214-256); the library
+ * borrows the pointers and writes in place.  An mc_env handle owns only
+ * small internal buffers (flag words, decode scratch, one template world).
+ *
+ * Threading: a handle may be used by one host thread at a time.  Different
+ * handles are independent (the reference's graph cache is process-global per
+ * mode, src/kernels.cu:2376-2382; here it is per handle).
+ */
+#ifndef MINECU_B200_H
+#define MINECU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC_ABI_VERSION 1
+
+/* status codes */
+#define MC_OK 0
+#define MC_ERR_INVALID (-1)     /* bad argument (size, pointer, alignment) */
+#define MC_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define MC_ERR_KERNEL (-3)      /* a kernel recorded an error (bounded wait expired) */
+#define MC_ERR_UNSUPPORTED (-4) /* configuration not supported by this build */
+
+/* numerics modes */
+#define MC_NUMERICS_REF_FAST 0 /* same fast-math CUDA calls and op order as the reference build */
+#define MC_NUMERICS_IEEE 1     /* IEEE-754 ops, bit-identical to the CPU checker */
+
+/* observation modes = MineEnv(obs_dtype=...) (minecu/__init__.py:162-169) */
+#define MC_OBS_FLOAT32 0
+#define MC_OBS_UINT8 1
+#define MC_OBS_UINT8_MINIMAL 2
+#define MC_OBS_UINT8_FP16 3
+#define MC_OBS_UINT8_PREBASIS 4
+#define MC_OBS_UINT8_PREBASIS_FULL 5
+#define MC_OBS_UINT8_SMEM 6
+#define MC_OBS_UINT8_FAST 7
+
+/* step forms */
+#define MC_FORM_PLAIN 0 /* one kernel per reference kernel, in the reference's order */
+#define MC_FORM_FUSED 1 /* one persistent kernel per step */
+
+/* Constructor arguments of MineEnv (minecu/__init__.py:141-165). */
+typedef struct mc_env_config {
+    int32_t batch_size;
+    int32_t world_x, world_y, world_z;
+    int32_t render_width, render_height;
+    int32_t max_steps;
+    float view_distance;
+    float fov_degrees;
+    float dt;
+    float gravity;
+    float walk_speed;
+    float sprint_mult;
+    float jump_vel;
+    int32_t ground_height;
+    int32_t target_block; /* -128..127, int8 semantics as the reference */
+    float reward_value;
+    int32_t has_episode_limit; /* 0 = episode_length None */
+    int32_t episode_length;
+    int32_t obs_mode;  /* MC_OBS_* */
+    int32_t numerics;  /* MC_NUMERICS_* */
+    float look_delta;  /* radians per discrete look action */
+    /* 0: spawn at (world_x/2, ground_height+2, world_z/2) as MineEnv does
+     * (minecu/__init__.py:195-198); 1: use spawn_x/y/z, as the reference's
+     * launchers take them (src/kernels.cu:2497-2520) */
+    int32_t spawn_override;
+    float spawn_x, spawn_y, spawn_z;
+} mc_env_config;
+
+/* State buffers (device pointers), the MineEnv attributes of
+ * minecu/__init__.py:214-256.  dbg_* are optional debug outputs the
+ * reference keeps internal: the voxel index the interaction touched per env
+ * (-1 none) and per pixel (hit_block + 1) | ((hit_face + 1) << 8). */
+typedef struct mc_env_state {
+    int8_t* voxels;      /* [B, Y, X, Z] */
+    float* positions;    /* [B, 3] */
+    float* velocities;   /* [B, 3] */
+    float* yaws;         /* [B] */
+    float* pitches;      /* [B] */
+    uint8_t* on_ground;  /* [B] (torch.bool) */
+    int32_t* step_count; /* [B] */
+    uint8_t* do_reset;   /* [B] (torch.bool) */
+    float* cameras;      /* [B, 5] */
+    float* basis;        /* [B, 14] for the prebasis modes, else NULL */
+    void* obs;           /* [B, H, W, 3] uint8 or float32 */
+    float* rewards;      /* [B] */
+    int32_t* dbg_interact; /* [B] or NULL */
+    int16_t* dbg_pixel;    /* [B, H, W] or NULL */
+} mc_env_state;
+
+typedef struct mc_env mc_env;
+
+/* Launch shape of the fused kernel (see mc_env_set_fused_config). */
+typedef struct mc_fused_config {
+    int32_t stage;         /* 1: bulk-copy each marched world into shared memory */
+    int32_t warps_per_cta; /* 4 or 8 */
+    int32_t ctas_per_sm;   /* persistent grid = SMs x ctas_per_sm */
+    int32_t px_per_lane;   /* 1, 2 or 4 pixels per lane per chunk */
+} mc_fused_config;
+
+/* ---- library ---------------------------------------------------------- */
+int mc_abi_version(void);
+/* Message of the last failed call on this host thread. */
+const char* mc_last_error(void);
+
+/* ---- env handle: MineEnv (minecu/__init__.py:65-479) ------------------ */
+/* Replaces MineEnv.__init__'s native half (minecu/__init__.py:141-212). */
+int mc_env_create(const mc_env_config* cfg, const mc_env_state* state, mc_env** out);
+int mc_env_destroy(mc_env* env);
+/* Re-point the borrowed state buffers (same sizes). */
+int mc_env_set_state(mc_env* env, const mc_env_state* state);
+/* MineEnv._generate_world (minecu/__init__.py:258-268): every world. */
+int mc_env_generate_world(mc_env* env, void* stream);
+/* MineEnv.reset(mask) (minecu/__init__.py:270-302); mask = device bool[B]
+ * or NULL for all.  No host synchronisation: the "any env reset" test of
+ * the reference (mask.any()) runs on the device. */
+int mc_env_reset(mc_env* env, const uint8_t* mask, void* stream);
+/* MineEnv.step(buttons int8[B,8], look float32[B,2]) (minecu/__init__.py:304-444),
+ * including the all-world regeneration when any env is done. */
+int mc_env_step(mc_env* env, const int8_t* buttons, const float* look, int form, void* stream);
+/* The discrete form step(actions) of docs/environment.md:5-17: actions
+ * uint8[B] in 0..10, look step = config.look_delta. */
+int mc_env_step_discrete(mc_env* env, const uint8_t* actions, int form, void* stream);
+/* MineEnv.get_obs / _render (minecu/__init__.py:446-472). */
+int mc_env_render(mc_env* env, void* stream);
+/* K fused steps of discrete actions actions[K,B] captured once in a CUDA
+ * graph and replayed; rewards_out / dones_out ([K,B], optional) receive each
+ * step's rewards and dones.  The graph is cached per (actions, outputs, K). */
+int mc_env_rollout(mc_env* env, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
+                   void* stream);
+/* Capture (and cache) the rollout graph without running it. */
+int mc_env_rollout_prepare(mc_env* env, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out);
+int mc_env_set_fused_config(mc_env* env, const mc_fused_config* cfg);
+int mc_env_get_fused_config(const mc_env* env, mc_fused_config* cfg);
+/* Reads and clears the device error word (synchronises the stream). */
+int mc_env_check_error(mc_env* env, void* stream);
+/* Bytes of dynamic shared memory the fused kernel uses per CTA. */
+int64_t mc_env_fused_smem_bytes(const mc_env* env);
+
+/* ---- stateless kernels: the reference's _C functions ------------------ */
+/* generate_world_kernel (src/kernels.cu:1793-1828) via launch_generate_world
+ * (src/kernels.cu:2281-2290); the seed is unused, as in the reference. */
+int mc_generate_world(int8_t* voxels, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t ground_height,
+                      uint32_t seed, void* stream);
+/* launch_place_tree (src/kernels.cu:2292-2301) */
+int mc_place_tree(int8_t* voxels, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t tree_x, int32_t tree_z,
+                  int32_t ground_height, void* stream);
+/* launch_place_house (src/kernels.cu:2303-2312) */
+int mc_place_house(int8_t* voxels, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t house_x,
+                   int32_t house_z, int32_t ground_height, void* stream);
+/* launch_reset (src/kernels.cu:2268-2279) */
+int mc_reset_agents(float* positions, float* velocities, float* yaws, float* pitches, uint8_t* on_ground,
+                    const uint8_t* do_reset, int32_t B, float spawn_x, float spawn_y, float spawn_z, void* stream);
+/* launch_render / launch_render_uint8 / _minimal / _fp16 / _fast
+ * (src/kernels.cu:2078-2160): render every env of `state` from
+ * state->cameras with the render family of cfg->obs_mode (shaded for
+ * float32/uint8/uint8_fast, flat otherwise). */
+int mc_render(const mc_env_config* cfg, const mc_env_state* state, int32_t shaded, void* stream);
+/* launch_precompute_camera_basis (src/kernels.cu:2162-2170) */
+int mc_precompute_camera_basis(const float* cameras, float* basis, int32_t B, int32_t width, int32_t height,
+                               float fov_degrees, int32_t numerics, void* stream);
+/* launch_render_uint8_prebasis (src/kernels.cu:2172-2190), non-cubic */
+int mc_render_uint8_prebasis(const int8_t* voxels, const float* basis, uint8_t* out, int32_t B, int32_t wx,
+                             int32_t wy, int32_t wz, int32_t width, int32_t height, int32_t max_steps,
+                             int32_t numerics, void* stream);
+/* launch_render_uint8_coalesced (src/kernels.cu:2212-2232): [Y,X,Z,B] voxels */
+int mc_render_uint8_coalesced(const int8_t* voxels_yxzb, const float* basis, uint8_t* out, int32_t B,
+                              int32_t world_size, int32_t width, int32_t height, int32_t max_steps,
+                              int32_t numerics, void* stream);
+/* The reference's 8 action-decode buffers (MineEnv.forward_in ...,
+ * minecu/__init__.py:242-250), written by decode_actions_kernel. */
+typedef struct mc_decode_buffers {
+    float* forward_in;
+    float* strafe_in;
+    float* delta_yaw_in;
+    float* delta_pitch_in;
+    uint8_t* jump_in;
+    uint8_t* do_break;
+    uint8_t* do_place;
+    float* speed_mult;
+} mc_decode_buffers;
+
+/* One step of the reference's _C.step / step_uint8 / _minimal / _fp16 /
+ * _fast / _prebasis / _prebasis_full / _smem (launch_step*,
+ * src/kernels.cu:2497-3243): kernels only, no world regeneration.  For
+ * every mode but prebasis_full, do_reset is an input and step_count is not
+ * touched (their episode logic runs in Python, minecu/__init__.py:363-366,
+ * 435-436); for prebasis_full the episode check and counter update run in
+ * the step.  The plain form writes the decode buffers as the reference
+ * does (dec must be non-NULL); the fused form keeps them in registers. */
+int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* state, const int8_t* buttons,
+                      const float* look, const mc_decode_buffers* dec, int32_t form, void* stream);
+/* launch_physics (src/kernels.cu:2234-2250) from the 8 decode inputs */
+int mc_physics(float* positions, float* velocities, float* yaws, float* pitches, uint8_t* on_ground,
+               const float* forward_in, const float* strafe_in, const float* delta_yaw_in,
+               const float* delta_pitch_in, const uint8_t* jump_in, const float* speed_mult, int32_t B,
+               int32_t world_size, float dt, float gravity, float walk_speed, float jump_vel, int32_t numerics,
+               void* stream);
+/* launch_raycast_break (src/kernels.cu:2252-2266) */
+int mc_raycast_break(int8_t* voxels, const float* positions, const float* yaws, const float* pitches,
+                     const uint8_t* do_break, float* rewards, int32_t B, int32_t world_size, int32_t target_block,
+                     float reward_value, int32_t numerics, void* stream);
+
+/* ---- synthetic action stream (no reference counterpart: the benchmark's
+ *      seeded Philox4x32-10 actions, docs/environment.md:5-17 table) ----- */
+int mc_philox_actions(uint8_t* actions, int32_t B, int32_t K, int32_t env_offset, int32_t step0, uint64_t seed,
+                      int32_t break_half, void* stream);
+int mc_discrete_to_buttons(const uint8_t* actions, int32_t B, float look_delta, int8_t* buttons, float* look,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MINECU_B200_H */

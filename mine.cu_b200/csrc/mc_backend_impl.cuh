@@ -1,0 +1,1325 @@
+// mc_backend_impl.cuh - the environment step for one numerics mode.
+//
+// Included by exactly two translation units:
+//   mc_fast.cu  (MC_NUMERICS_FAST=1, nvcc --use_fast_math): calls the same
+//               CUDA math functions as the reference build, in the same op
+//               order, so results match the reference bit for bit;
+//   mc_ieee.cu  (MC_NUMERICS_FAST=0, -fmad=false): IEEE-754 ops and the trig
+//               of mc_ieee_math.h, so results match the CPU checker bit for bit.
+// MC_NS names the namespace so both back ends link into one library.
+//
+// Semantics follow the reference's src/kernels.cu; every device function
+// cites the lines it restates.  Two launch forms share these functions:
+//   plain : one kernel per reference kernel, in the reference's order;
+//   fused : one persistent kernel per step, a warp per env.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include "mc_internal.h"
+#include "mc_ieee_math.h"
+#include "mc_philox.h"
+
+#ifndef MC_NS
+#error "define MC_NS before including mc_backend_impl.cuh"
+#endif
+
+namespace MC_NS {
+
+constexpr int8_t AIR = -1, GRASS = 0, DIRT = 1, OAKLOG = 3, LEAVES = 4, BRICK = 8,
+                 COBBLESTONE = 9, PLANKS = 10, BEDROCK = 12;
+
+// Colour tables: the reference's BLOCK_COLORS / SKY_COLOR (kernels.cu:27-44)
+// and the pre-rounded BLOCK_COLORS_U8 / SKY_COLOR_U8 (kernels.cu:479-495).
+__constant__ float c_rgb[13][3] = {
+    {0.30f, 0.65f, 0.20f}, {0.55f, 0.35f, 0.20f}, {0.50f, 0.50f, 0.50f}, {0.55f, 0.40f, 0.25f},
+    {0.20f, 0.55f, 0.15f}, {0.90f, 0.85f, 0.60f}, {0.20f, 0.40f, 0.80f}, {0.85f, 0.90f, 0.95f},
+    {0.70f, 0.35f, 0.30f}, {0.40f, 0.40f, 0.40f}, {0.75f, 0.60f, 0.40f}, {0.95f, 0.95f, 0.98f},
+    {0.15f, 0.15f, 0.15f}};
+__constant__ float c_sky[3] = {0.53f, 0.81f, 0.92f};
+__constant__ uint8_t c_rgb8[13][3] = {
+    {76, 166, 51}, {140, 89, 51}, {127, 127, 127}, {140, 102, 64}, {51, 140, 38},
+    {229, 217, 153}, {51, 102, 204}, {217, 229, 242}, {178, 89, 76}, {102, 102, 102},
+    {191, 153, 102}, {242, 242, 250}, {38, 38, 38}};
+__constant__ uint8_t c_sky8[3] = {135, 206, 235};
+
+// ---------------------------------------------------------------------------
+// Numerics policy
+// ---------------------------------------------------------------------------
+#if MC_NUMERICS_FAST
+struct N {
+    static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    static __device__ __forceinline__ float cos(float x) { return cosf(x); }
+    static __device__ __forceinline__ float tan(float x) { return tanf(x); }
+    static __device__ __forceinline__ void sincos_i(float x, float* s, float* c) { __sincosf(x, s, c); }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+};
+#else
+struct N {
+    static __device__ __forceinline__ float sin(float x) { return mc_ieee_sinf(x); }
+    static __device__ __forceinline__ float cos(float x) { return mc_ieee_cosf(x); }
+    static __device__ __forceinline__ float tan(float x) { return mc_ieee_tanf(x); }
+    static __device__ __forceinline__ void sincos_i(float x, float* s, float* c) { mc_ieee_sincosf(x, s, c); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float sqrt(float x) { return __fsqrt_rn(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
+};
+#endif
+
+// ---------------------------------------------------------------------------
+// Agent step
+// ---------------------------------------------------------------------------
+struct Dec {
+    float fwd, strafe, dyaw, dpitch, speed;
+    bool jump, brk, place;
+};
+
+// decode_actions_kernel (kernels.cu:1459-1504)
+__device__ __forceinline__ Dec decode_buttons(const int8_t b[8], float l0, float l1, float sprint_mult) {
+    Dec d;
+    d.fwd = (float)b[0] - (float)b[1];
+    d.strafe = (float)b[3] - (float)b[2];
+    d.dyaw = l0;
+    d.dpitch = l1;
+    d.jump = (b[4] != 0);
+    d.brk = (b[5] != 0);
+    d.place = (b[6] != 0);
+    d.speed = (b[0] && b[7]) ? sprint_mult : 1.0f;
+    return d;
+}
+
+__device__ __forceinline__ void load_action(const mc_kp& p, long long i, int8_t b[8], float& l0, float& l1) {
+    if (p.actions) {
+        float lk[2];
+        mc_discrete_to_buttons(p.actions[i], p.look_delta, b, lk);
+        l0 = lk[0];
+        l1 = lk[1];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) b[k] = p.buttons[i * 8 + k];
+        l0 = p.look[i * 2 + 0];
+        l1 = p.look[i * 2 + 1];
+    }
+}
+
+struct Agent {
+    float x, y, z, vx, vy, vz, yaw, pitch;
+    bool og;
+};
+
+__device__ __forceinline__ Agent load_agent(const mc_kp& p, long long i) {
+    Agent a;
+    a.x = p.positions[i * 3 + 0];
+    a.y = p.positions[i * 3 + 1];
+    a.z = p.positions[i * 3 + 2];
+    a.vx = p.velocities[i * 3 + 0];
+    a.vy = p.velocities[i * 3 + 1];
+    a.vz = p.velocities[i * 3 + 2];
+    a.yaw = p.yaws[i];
+    a.pitch = p.pitches[i];
+    a.og = p.on_ground[i] != 0;
+    return a;
+}
+
+__device__ __forceinline__ void store_agent(const mc_kp& p, long long i, const Agent& a) {
+    p.positions[i * 3 + 0] = a.x;
+    p.positions[i * 3 + 1] = a.y;
+    p.positions[i * 3 + 2] = a.z;
+    p.velocities[i * 3 + 0] = a.vx;
+    p.velocities[i * 3 + 1] = a.vy;
+    p.velocities[i * 3 + 2] = a.vz;
+    p.yaws[i] = a.yaw;
+    p.pitches[i] = a.pitch;
+    p.on_ground[i] = a.og ? 1 : 0;
+}
+
+// physics_kernel (kernels.cu:1511-1584): rotate, walk, gravity, clamp to the
+// flat ground at world_y/4 and to [1, W-1] in x and z.  No voxel collision.
+__device__ __forceinline__ void physics(Agent& a, const Dec& d, const mc_kp& p) {
+    a.yaw = a.yaw + d.dyaw;
+    float new_pitch = a.pitch + d.dpitch;
+    a.pitch = fminf(fmaxf(new_pitch, -1.56f), 1.56f);
+    float cos_yaw = N::cos(a.yaw);
+    float sin_yaw = N::sin(a.yaw);
+    float fwd = d.fwd, str = d.strafe;
+    float speed = p.walk_speed * d.speed;
+    float move_x = sin_yaw * fwd * speed * p.dt + cos_yaw * str * p.walk_speed * p.dt;
+    float move_z = cos_yaw * fwd * speed * p.dt - sin_yaw * str * p.walk_speed * p.dt;
+    float vel_y = a.vy;
+    if (d.jump && a.og) vel_y = p.jump_vel;
+    vel_y += p.gravity * p.dt;
+    float new_x = a.x + move_x;
+    float new_y = a.y + vel_y * p.dt;
+    float new_z = a.z + move_z;
+    float ground_y = (float)(p.wy / 4);
+    if (new_y <= ground_y) {
+        new_y = ground_y;
+        vel_y = 0.0f;
+        a.og = true;
+    } else {
+        a.og = false;
+    }
+    float margin = 1.0f;
+    new_x = fminf(fmaxf(new_x, margin), (float)p.wx - margin);
+    new_z = fminf(fmaxf(new_z, margin), (float)p.wz - margin);
+    a.x = new_x;
+    a.y = new_y;
+    a.z = new_z;
+    a.vy = vel_y;
+}
+
+// reset_kernel (kernels.cu:1760-1786)
+__device__ __forceinline__ void reset_agent(Agent& a, const mc_kp& p) {
+    a.x = p.spawn_x;
+    a.y = p.spawn_y;
+    a.z = p.spawn_z;
+    a.vx = 0.0f;
+    a.vy = 0.0f;
+    a.vz = 0.0f;
+    a.yaw = 0.0f;
+    a.pitch = 0.0f;
+    a.og = false;
+}
+
+// episode_check_kernel (kernels.cu:1954-1968) and the Python rule of
+// minecu/__init__.py:363-366.
+__device__ __forceinline__ bool episode_done(const mc_kp& p, int32_t cnt) {
+    if (p.episode_rule == 0) return p.has_limit && cnt >= p.episode_length;
+    return p.episode_length > 0 && cnt >= p.episode_length;
+}
+
+// One interact sample k of raycast_interact_kernel (kernels.cu:1621-1653):
+// the point at t = 0.1 + k * 4/32 along the view direction from the eye.
+struct Sample {
+    int idx;  // flat in-env voxel index, valid if inb
+    bool inb;
+};
+__device__ __forceinline__ Sample interact_sample(int k, float eye_x, float eye_y, float eye_z,
+                                                  float dir_x, float dir_y, float dir_z,
+                                                  int wx, int wy, int wz) {
+    float reach = 4.0f;
+    float t = 0.1f + k * (reach / 32.0f);
+    float px = eye_x + dir_x * t;
+    float py = eye_y + dir_y * t;
+    float pz = eye_z + dir_z * t;
+    int vx = (int)floorf(px);
+    int vy = (int)floorf(py);
+    int vz = (int)floorf(pz);
+    Sample s;
+    s.inb = (vx >= 0 && vx < wx && vy >= 0 && vy < wy && vz >= 0 && vz < wz);
+    s.idx = vy * (wx * wz) + vx * wz + vz;
+    return s;
+}
+
+__device__ __forceinline__ void interact_dir(const Agent& a, float& dx, float& dy, float& dz) {
+    float cos_yaw = N::cos(a.yaw);
+    float sin_yaw = N::sin(a.yaw);
+    float cos_pitch = N::cos(a.pitch);
+    float sin_pitch = N::sin(a.pitch);
+    dx = sin_yaw * cos_pitch;
+    dy = sin_pitch;
+    dz = cos_yaw * cos_pitch;
+}
+
+__device__ __forceinline__ bool reward_hit(const mc_kp& p, int8_t blk) {
+    int8_t target = (int8_t)p.target_block;
+    return target < 0 || blk == target;
+}
+
+// raycast_interact_kernel (kernels.cu:1591-1680), one thread per env.
+// Returns the in-env index written (-1 if none); *reward as the reference.
+__device__ __forceinline__ int interact_seq(int8_t* w, const Agent& a, bool brk, bool place,
+                                            const mc_kp& p, float* reward) {
+    *reward = 0.0f;
+    if (!brk && !place) return -1;
+    float dx, dy, dz;
+    interact_dir(a, dx, dy, dz);
+    float eye_x = a.x, eye_y = a.y + 1.6f, eye_z = a.z;
+    int prev = -1;
+    for (int k = 0; k < 32; ++k) {
+        Sample s = interact_sample(k, eye_x, eye_y, eye_z, dx, dy, dz, p.wx, p.wy, p.wz);
+        if (s.inb) {
+            int8_t blk = w[s.idx];
+            if (blk >= 0) {
+                if (brk) {
+                    if (reward_hit(p, blk)) *reward = p.reward_value;
+                    w[s.idx] = AIR;
+                    return s.idx;
+                } else if (place && prev >= 0) {
+                    w[prev] = DIRT;
+                    return prev;
+                }
+                return -1;
+            }
+            prev = s.idx;
+        }
+    }
+    return -1;
+}
+
+// The same interaction with the 32 samples spread over the 32 lanes of a
+// warp: the first in-bounds solid sample is the lowest set bit of a ballot
+// and the placement voxel is the highest in-bounds sample below it, which is
+// exactly what the reference's sequential loop selects.  Must be called by
+// all 32 lanes.  Returns the in-env index written (-1 if none), uniform
+// across the warp; *mod_val gets the value written.
+__device__ __forceinline__ int interact_warp(int8_t* w, const Agent& a, bool brk, bool place,
+                                             const mc_kp& p, int lane, float* reward, int8_t* mod_val) {
+    *reward = 0.0f;
+    *mod_val = 0;
+    if (!brk && !place) return -1;  // warp-uniform
+    float dx, dy, dz;
+    interact_dir(a, dx, dy, dz);
+    Sample s = interact_sample(lane, a.x, a.y + 1.6f, a.z, dx, dy, dz, p.wx, p.wy, p.wz);
+    int8_t blk = s.inb ? w[s.idx] : AIR;
+    unsigned solid = __ballot_sync(0xffffffffu, s.inb && blk >= 0);
+    unsigned inbm = __ballot_sync(0xffffffffu, s.inb);
+    if (solid == 0u) return -1;
+    int first = __ffs(solid) - 1;
+    if (brk) {
+        int8_t hb = (int8_t)__shfl_sync(0xffffffffu, (int)blk, first);
+        int hidx = __shfl_sync(0xffffffffu, s.idx, first);
+        if (reward_hit(p, hb)) *reward = p.reward_value;
+        if (lane == first) w[s.idx] = AIR;
+        *mod_val = AIR;
+        return hidx;
+    }
+    unsigned before = inbm & ((1u << first) - 1u);
+    if (before == 0u) return -1;
+    int pl = 31 - __clz(before);
+    int pidx = __shfl_sync(0xffffffffu, s.idx, pl);
+    if (lane == pl) w[s.idx] = DIRT;
+    *mod_val = DIRT;
+    return pidx;
+}
+
+// ---------------------------------------------------------------------------
+// Render: per-env camera constants
+// ---------------------------------------------------------------------------
+struct Cam {
+    float eye_x, eye_y, eye_z;
+    float fx, fy, fz, rx, rz, ux, uy, uz;
+};
+
+// Camera basis as the per-pixel code of render_kernel / _uint8 / _minimal /
+// _fp16 / _fast computes it (kernels.cu:113-136): cosf/sinf of yaw/pitch.
+// Pure function of the camera, so computing it once per env gives the bits
+// every pixel of the reference computes.
+__device__ __forceinline__ Cam cam_trig(float cx, float cy, float cz, float yaw, float pitch) {
+    Cam c;
+    c.eye_x = cx;
+    c.eye_y = cy + 1.6f;
+    c.eye_z = cz;
+    float cos_yaw = N::cos(yaw);
+    float sin_yaw = N::sin(yaw);
+    float cos_pitch = N::cos(pitch);
+    float sin_pitch = N::sin(pitch);
+    c.fx = sin_yaw * cos_pitch;
+    c.fy = sin_pitch;
+    c.fz = cos_yaw * cos_pitch;
+    c.rx = cos_yaw;
+    c.rz = -sin_yaw;
+    c.ux = -sin_yaw * sin_pitch;
+    c.uy = cos_pitch;
+    c.uz = -cos_yaw * sin_pitch;
+    return c;
+}
+
+// precompute_camera_basis_kernel (kernels.cu:511-561), all 13 written words.
+__device__ __forceinline__ void basis_compute(float cx, float cy, float cz, float yaw, float pitch,
+                                              int width, int height, float fov, float out[13]) {
+    float sin_yaw, cos_yaw, sin_pitch, cos_pitch;
+    N::sincos_i(yaw, &sin_yaw, &cos_yaw);
+    N::sincos_i(pitch, &sin_pitch, &cos_pitch);
+    float fov_rad = fov * 0.01745329f;
+    float half_fov = N::tan(fov_rad * 0.5f);
+    float aspect = N::div((float)width, (float)height);
+    out[0] = cx;
+    out[1] = cy + 1.6f;
+    out[2] = cz;
+    out[3] = sin_yaw * cos_pitch;
+    out[4] = sin_pitch;
+    out[5] = cos_yaw * cos_pitch;
+    out[6] = cos_yaw;
+    out[7] = -sin_yaw;
+    out[8] = -sin_yaw * sin_pitch;
+    out[9] = cos_pitch;
+    out[10] = -cos_yaw * sin_pitch;
+    out[11] = half_fov * aspect;
+    out[12] = half_fov;
+}
+
+// scale_u / scale_v of precompute_camera_basis_kernel (kernels.cu:541-559);
+// they do not depend on the camera.
+__device__ __forceinline__ void prebasis_scales(int width, int height, float fov, float* su, float* sv) {
+    float fov_rad = fov * 0.01745329f;
+    float half_fov = N::tan(fov_rad * 0.5f);
+    float aspect = N::div((float)width, (float)height);
+    *su = half_fov * aspect;
+    *sv = half_fov;
+}
+
+__device__ __forceinline__ Cam cam_from_basis(const float* b) {
+    Cam c;
+    c.eye_x = b[0]; c.eye_y = b[1]; c.eye_z = b[2];
+    c.fx = b[3]; c.fy = b[4]; c.fz = b[5];
+    c.rx = b[6]; c.rz = b[7];
+    c.ux = b[8]; c.uy = b[9]; c.uz = b[10];
+    return c;
+}
+
+// Per-column u and per-row v of each family.  They depend only on the pixel
+// coordinate and launch constants, so the fused kernel tabulates them.
+// Shaded family: kernels.cu:129-134 (fov_rad = fov * 3.14159265 / 180).
+__device__ __forceinline__ float u_shaded(int px, int width, int height, float fov) {
+    float fov_rad = fov * 3.14159265f / 180.0f;
+    float aspect = N::div((float)width, (float)height);
+    float half_fov = N::tan(fov_rad * 0.5f);
+    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * half_fov * aspect;
+}
+__device__ __forceinline__ float v_shaded(int py, int height, float fov) {
+    float fov_rad = fov * 3.14159265f / 180.0f;
+    float half_fov = N::tan(fov_rad * 0.5f);
+    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * half_fov;
+}
+// Minimal/fp16 family: kernels.cu:1029-1034 (fov_rad = fov * 0.01745329).
+__device__ __forceinline__ float u_minimal(int px, int width, int height, float fov) {
+    float fov_rad = fov * 0.01745329f;
+    float aspect = N::div((float)width, (float)height);
+    float half_fov = N::tan(fov_rad * 0.5f);
+    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * half_fov * aspect;
+}
+__device__ __forceinline__ float v_minimal(int py, int height, float fov) {
+    float fov_rad = fov * 0.01745329f;
+    float half_fov = N::tan(fov_rad * 0.5f);
+    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * half_fov;
+}
+// Prebasis family: kernels.cu:616-617 (scales from the basis).
+__device__ __forceinline__ float u_prebasis(int px, int width, float scale_u) {
+    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * scale_u;
+}
+__device__ __forceinline__ float v_prebasis(int py, int height, float scale_v) {
+    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * scale_v;
+}
+
+// Voxel sources for the ray march.
+struct VoxGlobal {
+    const int8_t* w;
+    __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+};
+struct VoxLdg {  // read-only world (plain render kernels): the reference's __ldg path
+    const int8_t* w;
+    __device__ __forceinline__ int8_t operator()(int idx) const { return __ldg(w + idx); }
+};
+struct VoxShared {
+    const int8_t* w;
+    __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+};
+
+struct Hit {
+    int blk;    // block id, -1 for sky
+    int face;   // -1 none, 0 x, 1 y, 2 z
+    float t;    // entry distance of the hit voxel (shaded family only)
+    int step_y; // sign of the ray's y (shaded shade rule)
+};
+
+// ray_intersects_aabb (kernels.cu:51-79) exit distance for a box [0, ws]^3
+// given the precomputed numerators (0 - eye) and (ws - eye).
+__device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float lo_x, float hi_x,
+                                           float lo_y, float hi_y, float lo_z, float hi_z, float* t_entry) {
+    float t1 = lo_x * ix, t2 = hi_x * ix;
+    float t3 = lo_y * iy, t4 = hi_y * iy;
+    float t5 = lo_z * iz, t6 = hi_z * iz;
+    *t_entry = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
+    return fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
+}
+
+// Shaded ray: ray setup, AABB early-out and DDA of render_kernel /
+// render_kernel_uint8 (kernels.cu:137-269) and, with FASTG, the ground
+// shortcut of render_kernel_uint8_fast (kernels.cu:1378-1405).  The
+// reference's cubic box [0, ws]^3 becomes [0,wx]x[0,wy]x[0,wz], which is the
+// same arithmetic when the world is cubic.  `inside` is a per-env flag: eye
+// strictly inside the box and view_distance >= 0;
+// then the AABB test always passes (t_entry < 0 <= view_distance) and its
+// exit distance is only computed if the march leaves the world.
+template <bool FASTG, class V>
+__device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
+                                         int max_steps, float vd, int gh, bool inside) {
+    float ray_x = c.fx + u * c.rx + v * c.ux;
+    float ray_y = c.fy + v * c.uy;
+    float ray_z = c.fz + u * c.rz + v * c.uz;
+    float ray_len = N::sqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
+    ray_x = N::div(ray_x, ray_len);
+    ray_y = N::div(ray_y, ray_len);
+    ray_z = N::div(ray_z, ray_len);
+
+    float ix = (ray_x != 0.0f) ? N::div(1.0f, ray_x) : 1e30f;
+    float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
+    float iz = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 1e30f;
+    float lo_x = 0.0f - c.eye_x, hi_x = (float)wx - c.eye_x;
+    float lo_y = 0.0f - c.eye_y, hi_y = (float)wy - c.eye_y;
+    float lo_z = 0.0f - c.eye_z, hi_z = (float)wz - c.eye_z;
+
+    Hit h;
+    h.step_y = (ray_y >= 0) ? 1 : -1;
+    h.blk = AIR;
+    h.face = -1;
+    h.t = 0.0f;
+    float t_exit = 0.0f;
+    bool have_exit = false;
+    if (!inside) {
+        float t_entry;
+        t_exit = aabb_exit(ix, iy, iz, lo_x, hi_x, lo_y, hi_y, lo_z, hi_z, &t_entry);
+        have_exit = true;
+        if (t_exit < 0 || t_entry > t_exit || t_entry > vd) return h;  // sky
+    }
+    int vx = (int)floorf(c.eye_x);
+    int vy = (int)floorf(c.eye_y);
+    int vz = (int)floorf(c.eye_z);
+    int sx = (ray_x >= 0) ? 1 : -1;
+    int sy = h.step_y;
+    int sz = (ray_z >= 0) ? 1 : -1;
+    float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
+    float tmx = (ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ix : ((float)vx - c.eye_x) * ix;
+    float tmy = (ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iy : ((float)vy - c.eye_y) * iy;
+    float tmz = (ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * iz : ((float)vz - c.eye_z) * iz;
+    float t = 0.0f;
+    int face = -1;
+    int wxz = wx * wz;
+    for (int step = 0; step < max_steps; ++step) {
+        if (t >= vd) break;
+        if (FASTG && vy < gh) {
+            h.blk = (vy == gh - 1) ? GRASS : DIRT;
+            break;
+        }
+        if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
+            int8_t b = vox(vy * wxz + vx * wz + vz);
+            if (b >= 0) {
+                h.blk = b;
+                break;
+            }
+        } else {
+            if (!have_exit) {
+                float t_entry;
+                t_exit = aabb_exit(ix, iy, iz, lo_x, hi_x, lo_y, hi_y, lo_z, hi_z, &t_entry);
+                have_exit = true;
+            }
+            if (t > t_exit) break;
+        }
+        if (tmx < tmy && tmx < tmz) {
+            t = tmx; tmx += tdx; vx += sx; face = 0;
+        } else if (tmy < tmz) {
+            t = tmy; tmy += tdy; vy += sy; face = 1;
+        } else {
+            t = tmz; tmz += tdz; vz += sz; face = 2;
+        }
+    }
+    h.face = face;
+    h.t = t;
+    return h;
+}
+
+__device__ __forceinline__ bool eye_inside(const Cam& c, int wx, int wy, int wz, float vd) {
+    return c.eye_x > 0.0f && c.eye_x < (float)wx && c.eye_y > 0.0f && c.eye_y < (float)wy &&
+           c.eye_z > 0.0f && c.eye_z < (float)wz && vd >= 0.0f;
+}
+
+// Shading and fog of the shaded family (kernels.cu:271-292, 446-469).
+__device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*rgb)[3], const float* sky, float out[3]) {
+    if (h.blk >= 0) {
+        float r = rgb[h.blk][0], g = rgb[h.blk][1], b_col = rgb[h.blk][2];
+        float shade = 1.0f;
+        if (h.face == 0) shade = 0.8f;
+        else if (h.face == 2) shade = 0.9f;
+        else if (h.face == 1 && h.step_y < 0) shade = 0.6f;
+        float fog = fminf(N::div(h.t, vd), 1.0f);
+        fog = fog * fog;
+        out[0] = r * shade * (1.0f - fog) + sky[0] * fog;
+        out[1] = g * shade * (1.0f - fog) + sky[1] * fog;
+        out[2] = b_col * shade * (1.0f - fog) + sky[2] * fog;
+    } else {
+        out[0] = sky[0];
+        out[1] = sky[1];
+        out[2] = sky[2];
+    }
+}
+
+__device__ __forceinline__ uint32_t to_u8(float x) { return (uint32_t)(uint8_t)(x * 255.0f); }
+
+// Flat ray of render_kernel_uint8_minimal / _prebasis / _smem
+// (kernels.cu:1036-1097, 619-679): rsqrtf normalisation, no AABB, no fog,
+// unsigned bounds test, non-cubic world.
+template <class V>
+__device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
+                                        int max_steps) {
+    float ray_x = c.fx + u * c.rx + v * c.ux;
+    float ray_y = c.fy + v * c.uy;
+    float ray_z = c.fz + u * c.rz + v * c.uz;
+    float ray_len = N::rsqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
+    ray_x *= ray_len;
+    ray_y *= ray_len;
+    ray_z *= ray_len;
+    int wxz = wx * wz;
+    int vx = (int)floorf(c.eye_x);
+    int vy = (int)floorf(c.eye_y);
+    int vz = (int)floorf(c.eye_z);
+    int sx = (ray_x >= 0) ? 1 : -1;
+    int sy = (ray_y >= 0) ? 1 : -1;
+    int sz = (ray_z >= 0) ? 1 : -1;
+    float ix = (ray_x != 0.0f) ? N::div(1.0f, ray_x) : 1e30f;
+    float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
+    float iz = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 1e30f;
+    float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
+    float tmx = (ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ix : ((float)vx - c.eye_x) * ix;
+    float tmy = (ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iy : ((float)vy - c.eye_y) * iy;
+    float tmz = (ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * iz : ((float)vz - c.eye_z) * iz;
+    Hit h;
+    h.blk = AIR;
+    h.face = -1;
+    h.t = 0.0f;
+    h.step_y = sy;
+    int face = -1;
+    for (int step = 0; step < max_steps; ++step) {
+        if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
+            int8_t b = vox(vy * wxz + vx * wz + vz);
+            if (b >= 0) {
+                h.blk = b;
+                break;
+            }
+        }
+        if (tmx < tmy && tmx < tmz) {
+            tmx += tdx; vx += sx; face = 0;
+        } else if (tmy < tmz) {
+            tmy += tdy; vy += sy; face = 1;
+        } else {
+            tmz += tdz; vz += sz; face = 2;
+        }
+    }
+    h.face = face;
+    return h;
+}
+
+// render_kernel_uint8_fp16 (kernels.cu:1176-1248): the DDA's t_max/t_delta
+// in binary16 (inverse 65504 for a zero component).
+template <class V>
+__device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
+                                        int max_steps) {
+    float ray_x = c.fx + u * c.rx + v * c.ux;
+    float ray_y = c.fy + v * c.uy;
+    float ray_z = c.fz + u * c.rz + v * c.uz;
+    float ray_len = N::rsqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
+    ray_x *= ray_len;
+    ray_y *= ray_len;
+    ray_z *= ray_len;
+    int wxz = wx * wz;
+    int vx = (int)floorf(c.eye_x);
+    int vy = (int)floorf(c.eye_y);
+    int vz = (int)floorf(c.eye_z);
+    int sx = (ray_x >= 0) ? 1 : -1;
+    int sy = (ray_y >= 0) ? 1 : -1;
+    int sz = (ray_z >= 0) ? 1 : -1;
+    float ixf = (ray_x != 0.0f) ? N::div(1.0f, ray_x) : 65504.0f;
+    float iyf = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 65504.0f;
+    float izf = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 65504.0f;
+    __half tdx = __float2half(fabsf(ixf));
+    __half tdy = __float2half(fabsf(iyf));
+    __half tdz = __float2half(fabsf(izf));
+    __half tmx = __float2half((ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ixf : ((float)vx - c.eye_x) * ixf);
+    __half tmy = __float2half((ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iyf : ((float)vy - c.eye_y) * iyf);
+    __half tmz = __float2half((ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * izf : ((float)vz - c.eye_z) * izf);
+    Hit h;
+    h.blk = AIR;
+    h.face = -1;
+    h.t = 0.0f;
+    h.step_y = sy;
+    int face = -1;
+    for (int step = 0; step < max_steps; ++step) {
+        if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
+            int8_t b = vox(vy * wxz + vx * wz + vz);
+            if (b >= 0) {
+                h.blk = b;
+                break;
+            }
+        }
+        if (__hlt(tmx, tmy) && __hlt(tmx, tmz)) {
+            tmx = __hadd(tmx, tdx); vx += sx; face = 0;
+        } else if (__hlt(tmy, tmz)) {
+            tmy = __hadd(tmy, tdy); vy += sy; face = 1;
+        } else {
+            tmz = __hadd(tmz, tdz); vz += sz; face = 2;
+        }
+    }
+    h.face = face;
+    return h;
+}
+
+__device__ __forceinline__ int16_t dbg_code(const Hit& h) { return (int16_t)((h.blk + 1) | ((h.face + 1) << 8)); }
+
+// ---------------------------------------------------------------------------
+// Plain form: one kernel per reference kernel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void flag_any(int32_t* flags, bool v) {
+    unsigned m = __ballot_sync(__activemask(), v);
+    if (m && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&flags[MC_FLAG_ANY_DONE], 1);
+}
+
+__global__ void k_episode_check(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    bool done = p.ext_done ? (p.do_reset[i] != 0) : episode_done(p, p.step_count[i]);
+    if (!p.ext_done) p.do_reset[i] = done ? 1 : 0;
+    flag_any(p.flags, done);
+}
+
+__global__ void k_decode(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    int8_t b[8];
+    float l0, l1;
+    load_action(p, i, b, l0, l1);
+    Dec d = decode_buttons(b, l0, l1, p.sprint_mult);
+    p.s_fwd[i] = d.fwd;
+    p.s_strafe[i] = d.strafe;
+    p.s_dyaw[i] = d.dyaw;
+    p.s_dpitch[i] = d.dpitch;
+    p.s_jump[i] = d.jump;
+    p.s_brk[i] = d.brk;
+    p.s_place[i] = d.place;
+    p.s_speed[i] = d.speed;
+}
+
+__device__ __forceinline__ Dec load_dec(const mc_kp& p, long long i) {
+    Dec d;
+    d.fwd = p.s_fwd[i];
+    d.strafe = p.s_strafe[i];
+    d.dyaw = p.s_dyaw[i];
+    d.dpitch = p.s_dpitch[i];
+    d.jump = p.s_jump[i] != 0;
+    d.brk = p.s_brk[i] != 0;
+    d.place = p.s_place[i] != 0;
+    d.speed = p.s_speed[i];
+    return d;
+}
+
+__global__ void k_physics(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    Agent a = load_agent(p, i);
+    physics(a, load_dec(p, i), p);
+    p.positions[i * 3 + 0] = a.x;
+    p.positions[i * 3 + 1] = a.y;
+    p.positions[i * 3 + 2] = a.z;
+    p.velocities[i * 3 + 1] = a.vy;
+    p.yaws[i] = a.yaw;
+    p.pitches[i] = a.pitch;
+    p.on_ground[i] = a.og ? 1 : 0;
+}
+
+// break_only: raycast_break_kernel (kernels.cu:1687-1753), no placement.
+__global__ void k_interact(mc_kp p, int break_only) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    Agent a = load_agent(p, i);
+    bool brk = p.s_brk[i] != 0;
+    bool place = break_only ? false : (p.s_place[i] != 0);
+    float reward;
+    long long wxyz = (long long)p.wx * p.wy * p.wz;
+    int idx = interact_seq(p.voxels + i * wxyz, a, brk, place, p, &reward);
+    p.rewards[i] = reward;
+    if (p.dbg_interact) p.dbg_interact[i] = idx;
+}
+
+__global__ void k_reset(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    if (p.do_reset[i]) {
+        Agent a;
+        reset_agent(a, p);
+        store_agent(p, i, a);
+    }
+}
+
+// episode_update_kernel (kernels.cu:1971-1986) == the Python counter update
+// of minecu/__init__.py:435-436.
+__global__ void k_episode_update(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B || p.ext_done) return;
+    p.step_count[i] = p.do_reset[i] ? 1 : p.step_count[i] + 1;
+}
+
+// update_cameras_kernel (kernels.cu:2320-2335)
+__global__ void k_cameras(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    p.cameras[i * 5 + 0] = p.positions[i * 3 + 0];
+    p.cameras[i * 5 + 1] = p.positions[i * 3 + 1];
+    p.cameras[i * 5 + 2] = p.positions[i * 3 + 2];
+    p.cameras[i * 5 + 3] = p.yaws[i];
+    p.cameras[i * 5 + 4] = p.pitches[i];
+}
+
+__global__ void k_basis(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    const float* cam = p.cameras + i * 5;
+    float out[13];
+    basis_compute(cam[0], cam[1], cam[2], cam[3], cam[4], p.W, p.H, p.fov, out);
+#pragma unroll
+    for (int k = 0; k < 13; ++k) p.basis[i * 14 + k] = out[k];
+}
+
+// Shaded render, one thread per pixel over B*H*W, as render_kernel /
+// render_kernel_uint8 / render_kernel_uint8_fast (1-D grid, 128 threads).
+template <bool FASTG, bool F32>
+__global__ void __launch_bounds__(128) k_render_shaded(mc_kp p) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long hw = (long long)p.H * p.W;
+    if (idx >= (long long)p.B * hw) return;
+    long long b = idx / hw;
+    int pix = (int)(idx - b * hw);
+    int py = pix / p.W, px = pix - py * p.W;
+    const float* cam = p.cameras + b * 5;
+    Cam c = cam_trig(__ldg(cam + 0), __ldg(cam + 1), __ldg(cam + 2), __ldg(cam + 3), __ldg(cam + 4));
+    bool inside = eye_inside(c, p.wx, p.wy, p.wz, p.vd);
+    float u = u_shaded(px, p.W, p.H, p.fov);
+    float v = v_shaded(py, p.H, p.fov);
+    VoxLdg vox{p.voxels + b * (long long)p.wx * p.wy * p.wz};
+    Hit h = shade_ray<FASTG>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
+    float rgb[3];
+    shade_rgb(h, p.vd, c_rgb, c_sky, rgb);
+    if (F32) {
+        float* o = (float*)p.obs + idx * 3;
+        o[0] = rgb[0]; o[1] = rgb[1]; o[2] = rgb[2];
+    } else {
+        uint8_t* o = (uint8_t*)p.obs + idx * 3;
+        o[0] = (uint8_t)to_u8(rgb[0]); o[1] = (uint8_t)to_u8(rgb[1]); o[2] = (uint8_t)to_u8(rgb[2]);
+    }
+    if (p.dbg_pixel) p.dbg_pixel[idx] = dbg_code(h);
+}
+
+// Flat render (minimal / fp16: 1-D grid over pixels with per-pixel trig;
+// prebasis: 2-D grid (pixel blocks, env) reading the [B,14] basis).
+template <int FAM>
+__global__ void __launch_bounds__(128) k_render_flat(mc_kp p) {
+    long long b;
+    int pix;
+    long long hw = (long long)p.H * p.W;
+    if (FAM == MC_FAM_PREBASIS) {
+        b = blockIdx.y;
+        pix = blockIdx.x * blockDim.x + threadIdx.x;
+        if (pix >= hw) return;
+    } else {
+        long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (idx >= (long long)p.B * hw) return;
+        b = idx / hw;
+        pix = (int)(idx - b * hw);
+    }
+    int py = pix / p.W, px = pix - py * p.W;
+    Cam c;
+    float u, v;
+    if (FAM == MC_FAM_PREBASIS) {
+        const float* bs = p.basis + b * 14;
+        float bb[13];
+#pragma unroll
+        for (int k = 0; k < 13; ++k) bb[k] = __ldg(bs + k);
+        c = cam_from_basis(bb);
+        u = u_prebasis(px, p.W, bb[11]);
+        v = v_prebasis(py, p.H, bb[12]);
+    } else {
+        const float* cam = p.cameras + b * 5;
+        c = cam_trig(__ldg(cam + 0), __ldg(cam + 1), __ldg(cam + 2), __ldg(cam + 3), __ldg(cam + 4));
+        u = u_minimal(px, p.W, p.H, p.fov);
+        v = v_minimal(py, p.H, p.fov);
+    }
+    long long wxyz = (long long)p.wx * p.wy * p.wz;
+    VoxLdg vox{p.voxels + b * wxyz};
+    Hit h;
+    if (FAM == MC_FAM_FP16) h = fp16_ray(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    else h = flat_ray(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    long long o = (b * hw + pix);
+    uint8_t* out = (uint8_t*)p.obs + o * 3;
+    const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
+    out[0] = col[0]; out[1] = col[1]; out[2] = col[2];
+    if (p.dbg_pixel) p.dbg_pixel[o] = dbg_code(h);
+}
+
+// render_kernel_uint8_coalesced (kernels.cu:709-826): prebasis semantics over
+// a [Y, X, Z, B] voxel layout, a warp = one pixel across 32 envs.
+__global__ void __launch_bounds__(128) k_render_coalesced(const int8_t* vox, const float* basis, uint8_t* out,
+                                                          int B, int ws, int W, int H, int max_steps) {
+    int pix = blockIdx.x;
+    int b = blockIdx.y * blockDim.x + threadIdx.x;
+    if (pix >= H * W || b >= B) return;
+    int py = pix / W, px = pix - py * W;
+    float bb[13];
+#pragma unroll
+    for (int k = 0; k < 13; ++k) bb[k] = __ldg(basis + (long long)b * 14 + k);
+    Cam c = cam_from_basis(bb);
+    float u = u_prebasis(px, W, bb[11]);
+    float v = v_prebasis(py, H, bb[12]);
+    struct VoxYXZB {
+        const int8_t* v;
+        int B, b, ws;
+        __device__ __forceinline__ int8_t operator()(int idx) const {
+            // idx = y*ws*ws + x*ws + z  ->  [y][x][z][b]
+            return __ldg(v + (long long)idx * B + b);
+        }
+    } acc{vox, B, b, ws};
+    Hit h = flat_ray(c, u, v, acc, ws, ws, ws, max_steps);
+    const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
+    uint8_t* o = out + ((long long)b * H * W + pix) * 3;
+    o[0] = col[0]; o[1] = col[1]; o[2] = col[2];
+}
+
+// ---------------------------------------------------------------------------
+// Fused form: one persistent kernel per step, one warp per env
+// ---------------------------------------------------------------------------
+// Shared memory layout (per CTA): u/v tables, colour tables, then per warp a
+// pixel staging buffer, an mbarrier and (stage=1) one world.
+struct FusedLayout {
+    int W, H;
+    int chunk_px;      // pixels per chunk (32 * px_per_lane)
+    int stage_bytes;   // staging bytes per warp
+    int world_bytes;   // world bytes per warp (0 when not staged)
+    int warp_bytes;    // total per warp (16-aligned)
+    int head_bytes;    // tables (16-aligned)
+};
+
+__host__ __device__ inline int mc_align16(int x) { return (x + 15) & ~15; }
+
+__host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int obs_f32, int stage, int ppl) {
+    FusedLayout L;
+    L.W = W;
+    L.H = H;
+    L.chunk_px = 32 * ppl;
+    L.stage_bytes = mc_align16(L.chunk_px * 3 * (obs_f32 ? 4 : 1));
+    L.world_bytes = stage ? mc_align16(wxyz) : 0;
+    L.warp_bytes = 16 + L.stage_bytes + L.world_bytes;  // 16: mbarrier
+    L.head_bytes = mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
+    return L;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait on an mbarrier phase; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Write `bytes` of a repeating 48-byte pattern (p0 p1 p2) to dst, lanes
+// strided.  dst must be 16-byte aligned and bytes a multiple of 16.
+__device__ __forceinline__ void fill_pattern16(uint8_t* dst, int bytes, uint4 p0, uint4 p1, uint4 p2, int lane) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    int n = bytes >> 4;
+    int m = lane % 3;  // (lane + 32 k) mod 3 advances by 2 per iteration
+    for (int k = lane; k < n; k += 32) {
+        d[k] = (m == 0) ? p0 : ((m == 1) ? p1 : p2);
+        m = (m + 2 >= 3) ? m - 1 : m + 2;
+    }
+}
+
+template <int FAM, bool F32, bool STAGE, int PPL>
+__global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int W = p.W, H = p.H;
+    const int HW = W * H;
+    const int wxz = p.wx * p.wz;
+    const int wxyz = wxz * p.wy;
+    FusedLayout L = fused_layout(W, H, wxyz, F32, STAGE, PPL);
+
+    // --- tables -------------------------------------------------------------
+    float* s_u = reinterpret_cast<float*>(smem);
+    float* s_v = s_u + W;
+    float (*s_rgb)[3] = reinterpret_cast<float (*)[3]>(s_v + H);
+    float* s_sky = reinterpret_cast<float*>(s_rgb + 13);
+    uint8_t (*s_rgb8)[3] = reinterpret_cast<uint8_t (*)[3]>(s_sky + 4);
+    uint8_t* s_sky8 = reinterpret_cast<uint8_t*>(s_rgb8 + 13);
+    float pb_su = 0.0f, pb_sv = 0.0f;
+    if (FAM == MC_FAM_PREBASIS) prebasis_scales(W, H, p.fov, &pb_su, &pb_sv);
+    for (int k = threadIdx.x; k < W; k += blockDim.x) {
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) s_u[k] = u_shaded(k, W, H, p.fov);
+        else if (FAM == MC_FAM_MINIMAL || FAM == MC_FAM_FP16) s_u[k] = u_minimal(k, W, H, p.fov);
+        else s_u[k] = u_prebasis(k, W, pb_su);
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) s_v[k] = v_shaded(k, H, p.fov);
+        else if (FAM == MC_FAM_MINIMAL || FAM == MC_FAM_FP16) s_v[k] = v_minimal(k, H, p.fov);
+        else s_v[k] = v_prebasis(k, H, pb_sv);
+    }
+    for (int k = threadIdx.x; k < 39; k += blockDim.x) {
+        s_rgb[k / 3][k % 3] = c_rgb[k / 3][k % 3];
+        s_rgb8[k / 3][k % 3] = c_rgb8[k / 3][k % 3];
+    }
+    if (threadIdx.x < 3) {
+        s_sky[threadIdx.x] = c_sky[threadIdx.x];
+        s_sky8[threadIdx.x] = c_sky8[threadIdx.x];
+    }
+    uint8_t* wbase = smem + L.head_bytes + warp * L.warp_bytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(wbase);
+    uint8_t* stage = wbase + 16;
+    int8_t* sworld = reinterpret_cast<int8_t*>(wbase + 16 + L.stage_bytes);
+    uint32_t mbar_a = smem_u32(mbar);
+    if (STAGE && lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    bool any_done = false;
+    bool failed = false;
+
+    const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
+    for (long long e = (long long)blockIdx.x * nwarps + warp; e < p.B && !failed;
+         e += (long long)gridDim.x * nwarps) {
+        // ---- agent step (every lane computes the same values) --------------
+        int8_t btn[8];
+        float l0, l1;
+        load_action(p, e, btn, l0, l1);
+        Dec d = decode_buttons(btn, l0, l1, p.sprint_mult);
+        int32_t cnt = p.ext_done ? 0 : p.step_count[e];
+        bool done = p.ext_done ? (p.do_reset[e] != 0) : episode_done(p, cnt);
+        Agent a = load_agent(p, e);
+        physics(a, d, p);
+        int8_t* gw = p.voxels + e * (long long)wxyz;
+        float reward;
+        int8_t mod_val;
+        int mod_idx = interact_warp(gw, a, d.brk, d.place, p, lane, &reward, &mod_val);
+        if (done) reset_agent(a, p);
+        any_done |= done;
+        if (lane == 0) {
+            store_agent(p, e, a);
+            if (!p.ext_done) {
+                p.step_count[e] = done ? 1 : cnt + 1;
+                p.do_reset[e] = done ? 1 : 0;
+            }
+            p.rewards[e] = reward;
+            p.cameras[e * 5 + 0] = a.x;
+            p.cameras[e * 5 + 1] = a.y;
+            p.cameras[e * 5 + 2] = a.z;
+            p.cameras[e * 5 + 3] = a.yaw;
+            p.cameras[e * 5 + 4] = a.pitch;
+            if (p.dbg_interact) p.dbg_interact[e] = mod_idx;
+        }
+        // ---- per-env render constants -------------------------------------
+        Cam c;
+        float bas[13];
+        if (FAM == MC_FAM_PREBASIS) {
+            basis_compute(a.x, a.y, a.z, a.yaw, a.pitch, W, H, p.fov, bas);
+            c = cam_from_basis(bas);
+            if (p.basis && lane == 0) {
+#pragma unroll
+                for (int k = 0; k < 13; ++k) p.basis[e * 14 + k] = bas[k];
+            }
+        } else {
+            c = cam_trig(a.x, a.y, a.z, a.yaw, a.pitch);
+        }
+        // Every ray starts in the eye's voxel.  If the first DDA step already
+        // hits (the eye is inside a solid voxel, or below ground for the
+        // ground-shortcut family), every pixel of the env gets the same
+        // colour, so the env is filled without marching.
+        const int ex = (int)floorf(c.eye_x), ey = (int)floorf(c.eye_y), ez = (int)floorf(c.eye_z);
+        bool eye_inb = (unsigned)ex < (unsigned)p.wx && (unsigned)ey < (unsigned)p.wy && (unsigned)ez < (unsigned)p.wz;
+        int eye_idx = ey * wxz + ex * p.wz + ez;
+        int8_t eye_blk = AIR;
+        __syncwarp();
+        if (eye_inb) eye_blk = gw[eye_idx];
+        bool inside = false;
+        bool buried;
+        int fill_blk = eye_blk;
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+            inside = eye_inside(c, p.wx, p.wy, p.wz, p.vd);
+            bool start_hit = eye_blk >= 0;
+            if (FAM == MC_FAM_SHADED_FAST && ey < p.gh) {
+                start_hit = true;
+                fill_blk = (ey == p.gh - 1) ? GRASS : DIRT;
+            }
+            buried = inside && p.vd > 0.0f && p.max_steps > 0 && start_hit;
+        } else {
+            buried = p.max_steps > 0 && eye_inb && eye_blk >= 0;
+        }
+        uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
+        const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
+        if (buried) {
+            Hit h;
+            h.blk = fill_blk;
+            h.face = -1;
+            h.t = 0.0f;
+            h.step_y = 1;
+            uint8_t bytes[12];
+            if (F32 || FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+                float rgb[3];
+                shade_rgb(h, p.vd, s_rgb, s_sky, rgb);
+                if (F32) {
+                    // pattern period 12 bytes
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        uint32_t w32 = __float_as_uint(rgb[k]);
+                        bytes[4 * k + 0] = (uint8_t)(w32);
+                        bytes[4 * k + 1] = (uint8_t)(w32 >> 8);
+                        bytes[4 * k + 2] = (uint8_t)(w32 >> 16);
+                        bytes[4 * k + 3] = (uint8_t)(w32 >> 24);
+                    }
+                } else {
+                    bytes[0] = (uint8_t)to_u8(rgb[0]);
+                    bytes[1] = (uint8_t)to_u8(rgb[1]);
+                    bytes[2] = (uint8_t)to_u8(rgb[2]);
+                }
+            } else {
+                bytes[0] = s_rgb8[fill_blk][0];
+                bytes[1] = s_rgb8[fill_blk][1];
+                bytes[2] = s_rgb8[fill_blk][2];
+            }
+            const int period = F32 ? 12 : 3;
+            if (vec_ok) {
+                uint32_t w[12];
+#pragma unroll
+                for (int k = 0; k < 12; ++k) {
+                    w[k] = (uint32_t)bytes[(4 * k + 0) % period] | ((uint32_t)bytes[(4 * k + 1) % period] << 8) |
+                           ((uint32_t)bytes[(4 * k + 2) % period] << 16) | ((uint32_t)bytes[(4 * k + 3) % period] << 24);
+                }
+                fill_pattern16(oenv, (int)obs_env_bytes, make_uint4(w[0], w[1], w[2], w[3]),
+                               make_uint4(w[4], w[5], w[6], w[7]), make_uint4(w[8], w[9], w[10], w[11]), lane);
+            } else {
+                for (long long k = lane; k < obs_env_bytes; k += 32) oenv[k] = bytes[k % period];
+            }
+            if (p.dbg_pixel) {
+                int16_t code = dbg_code(h);
+                for (int k = lane; k < HW; k += 32) p.dbg_pixel[e * HW + k] = code;
+            }
+            continue;
+        }
+        // ---- stage the world into shared memory ----------------------------
+        const int8_t* wsrc = gw;
+        if (STAGE) {
+            if (lane == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_a), "r"(wxyz)
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_u32(sworld)),
+                    "l"(gw), "r"(wxyz), "r"(mbar_a)
+                    : "memory");
+            }
+            bool ok = mbar_wait(mbar_a, phase);
+            phase ^= 1u;
+            if (!ok) {
+                if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
+                failed = true;
+                break;
+            }
+            // the interaction may have written after the copy read the byte
+            if (lane == 0 && mod_idx >= 0) sworld[mod_idx] = mod_val;
+            __syncwarp();
+            wsrc = sworld;
+        }
+        // ---- march every pixel ---------------------------------------------
+        const int nchunks = (HW + L.chunk_px - 1) / L.chunk_px;
+        for (int ch = 0; ch < nchunks; ++ch) {
+            const int base = ch * L.chunk_px;
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) {
+                const int pix = base + j * 32 + lane;
+                if (pix < HW) {
+                    const int py = pix / W;
+                    const int px = pix - py * W;
+                    Hit h;
+                    const float u = s_u[px];
+                    const float v = s_v[py];
+                    if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
+                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
+                    } else if (FAM == MC_FAM_FP16) {
+                        if (STAGE) h = fp16_ray(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        else h = fp16_ray(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                    } else {
+                        if (STAGE) h = flat_ray(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        else h = flat_ray(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                    }
+                    const int so = (j * 32 + lane);
+                    if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+                        float rgb[3];
+                        shade_rgb(h, p.vd, s_rgb, s_sky, rgb);
+                        if (F32) {
+                            float* sf = reinterpret_cast<float*>(stage) + so * 3;
+                            sf[0] = rgb[0]; sf[1] = rgb[1]; sf[2] = rgb[2];
+                        } else {
+                            uint8_t* sb = stage + so * 3;
+                            sb[0] = (uint8_t)to_u8(rgb[0]);
+                            sb[1] = (uint8_t)to_u8(rgb[1]);
+                            sb[2] = (uint8_t)to_u8(rgb[2]);
+                        }
+                    } else {
+                        const uint8_t* col = (h.blk >= 0) ? s_rgb8[h.blk] : s_sky8;
+                        uint8_t* sb = stage + so * 3;
+                        sb[0] = col[0]; sb[1] = col[1]; sb[2] = col[2];
+                    }
+                    if (p.dbg_pixel) p.dbg_pixel[e * HW + pix] = dbg_code(h);
+                }
+            }
+            __syncwarp();
+            // copy the chunk out
+            const int npx = min(L.chunk_px, HW - base);
+            const int nbytes = npx * 3 * (F32 ? 4 : 1);
+            uint8_t* dst = oenv + (long long)base * 3 * (F32 ? 4 : 1);
+            if (vec_ok && (nbytes & 15) == 0) {
+                const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+                uint4* d4 = reinterpret_cast<uint4*>(dst);
+                for (int k = lane; k < (nbytes >> 4); k += 32) d4[k] = s4[k];
+            } else {
+                for (int k = lane; k < nbytes; k += 32) dst[k] = stage[k];
+            }
+            __syncwarp();
+        }
+    }
+    if (__syncthreads_or(any_done ? 1 : 0) && threadIdx.x == 0) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static inline int grid_1d(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+static int render_launch(const mc_kp* p, int family, cudaStream_t s) {
+    long long total = (long long)p->B * p->H * p->W;
+    if (total == 0) return 0;
+    switch (family) {
+        case MC_FAM_SHADED:
+            if (p->obs_f32) k_render_shaded<false, true><<<grid_1d(total, 128), 128, 0, s>>>(*p);
+            else k_render_shaded<false, false><<<grid_1d(total, 128), 128, 0, s>>>(*p);
+            break;
+        case MC_FAM_SHADED_FAST:
+            k_render_shaded<true, false><<<grid_1d(total, 128), 128, 0, s>>>(*p);
+            break;
+        case MC_FAM_MINIMAL:
+            k_render_flat<MC_FAM_MINIMAL><<<grid_1d(total, 128), 128, 0, s>>>(*p);
+            break;
+        case MC_FAM_FP16:
+            k_render_flat<MC_FAM_FP16><<<grid_1d(total, 128), 128, 0, s>>>(*p);
+            break;
+        case MC_FAM_PREBASIS: {
+            dim3 g(grid_1d((long long)p->H * p->W, 128), p->B);
+            k_render_flat<MC_FAM_PREBASIS><<<g, 128, 0, s>>>(*p);
+            break;
+        }
+        default:
+            return (int)cudaErrorInvalidValue;
+    }
+    return (int)cudaGetLastError();
+}
+
+// The reference's step kernel sequence (kernels.cu:2457-2494, 2909-2991):
+// episode check, decode, physics, interact, reset, counter, cameras,
+// (basis), render.  World regeneration is launched by the caller.
+static int step_plain(const mc_kp* p, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    int gb = grid_1d(p->B, 256);
+    k_episode_check<<<gb, 256, 0, s>>>(*p);
+    k_decode<<<gb, 256, 0, s>>>(*p);
+    k_physics<<<gb, 256, 0, s>>>(*p);
+    k_interact<<<gb, 256, 0, s>>>(*p, 0);
+    k_reset<<<gb, 256, 0, s>>>(*p);
+    k_episode_update<<<gb, 256, 0, s>>>(*p);
+    k_cameras<<<gb, 256, 0, s>>>(*p);
+    if (p->family == MC_FAM_PREBASIS) k_basis<<<gb, 256, 0, s>>>(*p);
+    int rc = (int)cudaGetLastError();
+    if (rc) return rc;
+    return render_launch(p, p->family, s);
+}
+
+static size_t fused_smem(const mc_kp* p, const mc_fused_cfg* cfg) {
+    int wxyz = p->wx * p->wy * p->wz;
+    FusedLayout L = fused_layout(p->W, p->H, wxyz, p->obs_f32, cfg->stage, cfg->px_per_lane);
+    return (size_t)L.head_bytes + (size_t)cfg->warps_per_cta * L.warp_bytes;
+}
+
+template <int FAM, bool F32, bool STAGE, int PPL>
+static int launch_fused_t(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
+    auto kern = k_step_fused<FAM, F32, STAGE, PPL>;
+    size_t smem = fused_smem(p, cfg);
+    static size_t attr_set = 0;  // per instantiation
+    if (smem > 48 * 1024 && smem > attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        attr_set = smem;
+    }
+    int threads = 32 * cfg->warps_per_cta;
+    long long ctas_needed = ((long long)p->B + cfg->warps_per_cta - 1) / cfg->warps_per_cta;
+    long long grid = (long long)num_sms * (cfg->ctas_per_sm > 0 ? cfg->ctas_per_sm : 1);
+    if (grid > ctas_needed) grid = ctas_needed;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, threads, smem, s>>>(*p);
+    return (int)cudaGetLastError();
+}
+
+template <int FAM, bool F32>
+static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
+    const bool st = cfg->stage != 0;
+    switch (cfg->px_per_lane) {
+        case 1: return st ? launch_fused_t<FAM, F32, true, 1>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 1>(p, cfg, num_sms, s);
+        case 2: return st ? launch_fused_t<FAM, F32, true, 2>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 2>(p, cfg, num_sms, s);
+        default: return st ? launch_fused_t<FAM, F32, true, 4>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 4>(p, cfg, num_sms, s);
+    }
+}
+
+static int step_fused(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    switch (p->family) {
+        case MC_FAM_SHADED:
+            return p->obs_f32 ? launch_fused_f<MC_FAM_SHADED, true>(p, cfg, num_sms, s)
+                              : launch_fused_f<MC_FAM_SHADED, false>(p, cfg, num_sms, s);
+        case MC_FAM_SHADED_FAST: return launch_fused_f<MC_FAM_SHADED_FAST, false>(p, cfg, num_sms, s);
+        case MC_FAM_MINIMAL: return launch_fused_f<MC_FAM_MINIMAL, false>(p, cfg, num_sms, s);
+        case MC_FAM_FP16: return launch_fused_f<MC_FAM_FP16, false>(p, cfg, num_sms, s);
+        case MC_FAM_PREBASIS: return launch_fused_f<MC_FAM_PREBASIS, false>(p, cfg, num_sms, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+static int basis_launch(const mc_kp* p, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    k_basis<<<grid_1d(p->B, 256), 256, 0, s>>>(*p);
+    return (int)cudaGetLastError();
+}
+static int decode_launch(const mc_kp* p, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    k_decode<<<grid_1d(p->B, 256), 256, 0, s>>>(*p);
+    return (int)cudaGetLastError();
+}
+static int physics_launch(const mc_kp* p, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    k_physics<<<grid_1d(p->B, 256), 256, 0, s>>>(*p);
+    return (int)cudaGetLastError();
+}
+static int interact_launch(const mc_kp* p, int break_only, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    k_interact<<<grid_1d(p->B, 256), 256, 0, s>>>(*p, break_only);
+    return (int)cudaGetLastError();
+}
+static int coalesced_launch(const int8_t* vox, const float* basis, uint8_t* out, int B, int ws, int W, int H,
+                            int max_steps, cudaStream_t s) {
+    if (B == 0 || W * H == 0) return 0;
+    dim3 g(W * H, (B + 127) / 128);
+    k_render_coalesced<<<g, 128, 0, s>>>(vox, basis, out, B, ws, W, H, max_steps);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace MC_NS

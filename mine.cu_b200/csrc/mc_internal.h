@@ -1,0 +1,102 @@
+// mc_internal.h - parameter blocks shared by the host runtime and the two
+// numerics back ends (mc_fast.cu, mc_ieee.cu).  Not part of the public C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Render families: one per reference render kernel.
+enum {
+    MC_FAM_SHADED = 0,       // render_kernel / render_kernel_uint8 (kernels.cu:87-470)
+    MC_FAM_SHADED_FAST = 1,  // render_kernel_uint8_fast (kernels.cu:1268-1442)
+    MC_FAM_MINIMAL = 2,      // render_kernel_uint8_minimal (kernels.cu:985-1119)
+    MC_FAM_FP16 = 3,         // render_kernel_uint8_fp16 (kernels.cu:1127-1260)
+    MC_FAM_PREBASIS = 4,     // render_kernel_uint8_prebasis / _smem (kernels.cu:568-700, 835-982)
+};
+
+// Device flag words owned by an env handle.
+enum { MC_FLAG_ANY_DONE = 0, MC_FLAG_REGEN_CTR = 1, MC_FLAG_ERROR = 2, MC_FLAG_WORDS = 8 };
+
+// Error codes a kernel can record in flags[MC_FLAG_ERROR] (never a trap).
+enum { MC_KERR_NONE = 0, MC_KERR_TMA_TIMEOUT = 1 };
+
+// Everything one step launch needs, passed to kernels by value.
+struct mc_kp {
+    // sizes
+    int B, wx, wy, wz, W, H;
+    // parameters (MineEnv.__init__, minecu/__init__.py:141-165)
+    int max_steps;
+    float vd, fov, dt, gravity, walk_speed, sprint_mult, jump_vel;
+    int gh;
+    int target_block;  // int8 semantics
+    float reward_value;
+    float spawn_x, spawn_y, spawn_z;
+    int episode_rule;  // 0: python rule (has_limit && cnt >= L); 1: kernel rule (L > 0 && cnt >= L)
+    int ext_done;      // 1: do_reset is an input and step_count is not touched (the reference's
+                       //    _C.step* entry points, whose episode logic runs in Python)
+    int has_limit, episode_length;
+    int family;   // MC_FAM_*
+    int obs_f32;  // float32 obs (else uint8)
+    float look_delta;  // discrete-action look step (radians)
+    // state (device, borrowed from the caller)
+    int8_t* voxels;
+    float* positions;
+    float* velocities;
+    float* yaws;
+    float* pitches;
+    uint8_t* on_ground;
+    int32_t* step_count;
+    uint8_t* do_reset;
+    float* cameras;
+    float* basis;  // [B,14] for the prebasis family, else may be null
+    void* obs;
+    float* rewards;
+    int32_t* dbg_interact;  // optional
+    int16_t* dbg_pixel;     // optional
+    // actions: either buttons+look, or discrete actions
+    const int8_t* buttons;
+    const float* look;
+    const uint8_t* actions;
+    // plain-form decode scratch (the reference's 8 decode buffers)
+    float* s_fwd;
+    float* s_strafe;
+    float* s_dyaw;
+    float* s_dpitch;
+    uint8_t* s_jump;
+    uint8_t* s_brk;
+    uint8_t* s_place;
+    float* s_speed;
+    int32_t* flags;               // MC_FLAG_* words
+    const int8_t* world_template; // one generated world (wx*wy*wz bytes)
+};
+
+// Launch shape of the fused step kernel (chosen by the autotuner).
+struct mc_fused_cfg {
+    int stage;          // 1: copy each rendered world into shared memory with a bulk copy; 0: read voxels from L1/L2
+    int warps_per_cta;  // 4 or 8
+    int ctas_per_sm;    // persistent grid = SMs * ctas_per_sm
+    int px_per_lane;    // pixels per lane per chunk (1, 2, 4)
+};
+
+// One numerics back end (ref_fast or ieee).
+struct mc_backend {
+    const char* name;
+    int (*step_plain)(const mc_kp* p, cudaStream_t s);
+    int (*step_fused)(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s);
+    // shaded (f32/u8) or flat render of every env from p->cameras (or p->basis)
+    int (*render)(const mc_kp* p, int family, cudaStream_t s);
+    // stand-alone kernels of the reference's _C module
+    int (*basis)(const mc_kp* p, cudaStream_t s);
+    int (*decode)(const mc_kp* p, cudaStream_t s);
+    int (*physics)(const mc_kp* p, cudaStream_t s);
+    int (*interact)(const mc_kp* p, int break_only, cudaStream_t s);
+    int (*render_coalesced)(const int8_t* vox_yxzb, const float* basis, uint8_t* out, int B, int ws,
+                            int W, int H, int max_steps, cudaStream_t s);
+    size_t (*fused_smem_bytes)(const mc_kp* p, const mc_fused_cfg* cfg);
+};
+
+extern "C" const mc_backend* mc_backend_fast();
+extern "C" const mc_backend* mc_backend_ieee();
+
+// numerics-independent kernels (mc_runtime.cu)
+int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s);
+int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s);

@@ -1,0 +1,979 @@
+// mc_runtime.cu - host runtime and C-ABI of libminecu_b200.so.
+//
+// Owns what the reference keeps in Python or in process-global statics:
+// the env handle (minecu/__init__.py MineEnv), the world template and its
+// regeneration (minecu/__init__.py:258-268, 356-359, 439-442), masked
+// reset (minecu/__init__.py:270-302), CUDA-graph capture of fused rollouts
+// (the reference's StepGraphState, src/kernels.cu:2338-2382, which keys its
+// graph on 3 of the ~20 pointers it bakes in; here the cache key is every
+// pointer the graph uses), and argument checking (the reference checks only
+// device/dtype of a few tensors, src/bindings.cpp:223-228).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/minecu_b200.h"
+#include "mc_internal.h"
+#include "mc_philox.h"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512];
+
+static int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* what) {
+    return fail(MC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define MC_CK(call)                                            \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);    \
+    } while (0)
+
+static int backend_rc(int rc, const char* what) {
+    if (rc == 0) return MC_OK;
+    return cuda_fail((cudaError_t)rc, what);
+}
+
+extern "C" int mc_abi_version(void) { return MC_ABI_VERSION; }
+extern "C" const char* mc_last_error(void) { return g_err; }
+
+// ---------------------------------------------------------------------------
+// numerics-independent kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int8_t AIR = -1, GRASS = 0, DIRT = 1, OAKLOG = 3, LEAVES = 4, BRICK = 8, COBBLESTONE = 9,
+                 PLANKS = 10, BEDROCK = 12;
+
+// generate_world_kernel (kernels.cu:1793-1828): y=0 bedrock, 1 <= y < gh-1
+// dirt, y = gh-1 grass, air above.  One thread per (env, y, x) row of z.
+__global__ void k_generate_world(int8_t* vox, long long rows, int wx, int wy, int wz, int gh) {
+    long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    int y = (int)((r / wx) % wy);
+    int8_t blk = AIR;
+    if (y == 0) blk = BEDROCK;
+    else if (y < gh - 1) blk = DIRT;
+    else if (y == gh - 1) blk = GRASS;
+    int8_t* row = vox + r * wz;
+    for (int z = 0; z < wz; ++z) row[z] = blk;
+}
+
+// place_tree_kernel (kernels.cu:1831-1865)
+__global__ void k_place_tree(int8_t* vox, int B, int wx, int wy, int wz, int tx, int tz, int gh) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    long long wxz = (long long)wx * wz, wxyz = wxz * wy;
+    for (int dy = 0; dy < 3; ++dy) {
+        int y = gh + dy;
+        if (y < wy) vox[b * wxyz + y * wxz + (long long)tx * wz + tz] = OAKLOG;
+    }
+    int ly = gh + 3;
+    if (ly < wy) vox[b * wxyz + ly * wxz + (long long)tx * wz + tz] = LEAVES;
+}
+
+// place_house_kernel (kernels.cu:1868-1946)
+__device__ __forceinline__ void house_set(int8_t* w, int wx, int wy, int wz, int hx, int hz, int gh, int dy, int dx,
+                                          int dz, int8_t blk) {
+    int vx = hx + dx, vy = gh + dy, vz = hz + dz;
+    if (vx >= 0 && vx < wx && vy >= 0 && vy < wy && vz >= 0 && vz < wz)
+        w[(long long)vy * wx * wz + (long long)vx * wz + vz] = blk;
+}
+
+__global__ void k_place_house(int8_t* vox, int B, int wx, int wy, int wz, int hx, int hz, int gh) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const int W = 5, D = 4, H = 4;
+    int8_t* w = vox + (long long)b * wx * wy * wz;
+    for (int dx = 0; dx < W; ++dx)
+        for (int dz = 0; dz < D; ++dz) house_set(w, wx, wy, wz, hx, hz, gh, 0, dx, dz, COBBLESTONE);
+    for (int dy = 1; dy <= 3; ++dy) {
+        for (int dx = 0; dx < W; ++dx) {
+            if (dx == 2 && dy <= 2) continue;  // door
+            house_set(w, wx, wy, wz, hx, hz, gh, dy, dx, 0, PLANKS);
+        }
+        for (int dx = 0; dx < W; ++dx) house_set(w, wx, wy, wz, hx, hz, gh, dy, dx, D - 1, PLANKS);
+        for (int dz = 1; dz < D - 1; ++dz) house_set(w, wx, wy, wz, hx, hz, gh, dy, 0, dz, PLANKS);
+        for (int dz = 1; dz < D - 1; ++dz) house_set(w, wx, wy, wz, hx, hz, gh, dy, W - 1, dz, PLANKS);
+    }
+    for (int dy = 1; dy <= 3; ++dy) {
+        house_set(w, wx, wy, wz, hx, hz, gh, dy, 0, 0, OAKLOG);
+        house_set(w, wx, wy, wz, hx, hz, gh, dy, W - 1, 0, OAKLOG);
+        house_set(w, wx, wy, wz, hx, hz, gh, dy, 0, D - 1, OAKLOG);
+        house_set(w, wx, wy, wz, hx, hz, gh, dy, W - 1, D - 1, OAKLOG);
+    }
+    for (int dx = 0; dx < W; ++dx)
+        for (int dz = 0; dz < D; ++dz) house_set(w, wx, wy, wz, hx, hz, gh, H, dx, dz, BRICK);
+}
+
+// Regenerate every world from the template (generate + tree + house give the
+// same bytes for every env, so one generated world is broadcast).  With
+// `conditional`, nothing is written unless flags[ANY_DONE] is set.  The last
+// CTA to finish clears the flag for the next step; every CTA reads the flag
+// before it arrives on the counter, so no CTA can see the cleared value.
+__global__ void k_regen(int8_t* vox, const int8_t* tmpl, int B, int wxyz, int32_t* flags, int conditional) {
+    __shared__ int go;
+    if (threadIdx.x == 0) go = conditional ? (*(volatile int32_t*)&flags[MC_FLAG_ANY_DONE] != 0) : 1;
+    __syncthreads();
+    if (go) {
+        if ((wxyz & 15) == 0) {
+            const int n16 = wxyz >> 4;
+            const uint4* t4 = reinterpret_cast<const uint4*>(tmpl);
+            for (long long b = blockIdx.x; b < B; b += gridDim.x) {
+                uint4* d4 = reinterpret_cast<uint4*>(vox + b * (long long)wxyz);
+                for (int k = threadIdx.x; k < n16; k += blockDim.x) d4[k] = __ldg(t4 + k);
+            }
+        } else {
+            for (long long b = blockIdx.x; b < B; b += gridDim.x) {
+                int8_t* d = vox + b * (long long)wxyz;
+                for (int k = threadIdx.x; k < wxyz; k += blockDim.x) d[k] = tmpl[k];
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned prev = atomicAdd(reinterpret_cast<unsigned*>(&flags[MC_FLAG_REGEN_CTR]), 1u);
+        if (prev == gridDim.x - 1) {
+            flags[MC_FLAG_ANY_DONE] = 0;
+            flags[MC_FLAG_REGEN_CTR] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// MineEnv.reset(mask) steps 1-3 (minecu/__init__.py:286-294): do_reset =
+// mask (or all), reset_kernel on those envs (kernels.cu:1760-1786),
+// step_count = 0 there; and the `mask.any()` test as a device flag.
+__global__ void k_reset_masked(mc_kp p, const uint8_t* mask) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool m = false;
+    if (i < p.B) {
+        m = mask ? (mask[i] != 0) : true;
+        p.do_reset[i] = m ? 1 : 0;
+        if (m) {
+            p.positions[i * 3 + 0] = p.spawn_x;
+            p.positions[i * 3 + 1] = p.spawn_y;
+            p.positions[i * 3 + 2] = p.spawn_z;
+            p.velocities[i * 3 + 0] = 0.0f;
+            p.velocities[i * 3 + 1] = 0.0f;
+            p.velocities[i * 3 + 2] = 0.0f;
+            p.yaws[i] = 0.0f;
+            p.pitches[i] = 0.0f;
+            p.on_ground[i] = 0;
+            p.step_count[i] = 0;
+        }
+    }
+    unsigned any = __ballot_sync(0xffffffffu, m);
+    if (any && (threadIdx.x & 31) == 0) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
+}
+
+// reset_kernel (kernels.cu:1760-1786) as the stand-alone _C.reset
+__global__ void k_reset_agents(float* pos, float* vel, float* yaw, float* pitch, uint8_t* og, const uint8_t* dr,
+                               int B, float sx, float sy, float sz) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || !dr[i]) return;
+    pos[i * 3 + 0] = sx;
+    pos[i * 3 + 1] = sy;
+    pos[i * 3 + 2] = sz;
+    vel[i * 3 + 0] = 0.0f;
+    vel[i * 3 + 1] = 0.0f;
+    vel[i * 3 + 2] = 0.0f;
+    yaw[i] = 0.0f;
+    pitch[i] = 0.0f;
+    og[i] = 0;
+}
+
+// update_cameras_kernel (kernels.cu:2320-2335)
+__global__ void k_cameras_rt(mc_kp p) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.B) return;
+    p.cameras[i * 5 + 0] = p.positions[i * 3 + 0];
+    p.cameras[i * 5 + 1] = p.positions[i * 3 + 1];
+    p.cameras[i * 5 + 2] = p.positions[i * 3 + 2];
+    p.cameras[i * 5 + 3] = p.yaws[i];
+    p.cameras[i * 5 + 4] = p.pitches[i];
+}
+
+__global__ void k_philox(uint8_t* actions, int B, int K, int env_offset, int step0, uint64_t seed, int break_half) {
+    long long n = (long long)B * K;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(i / B), b = (int)(i - (long long)k * B);
+        actions[i] = mc_action_draw(seed, (uint32_t)(env_offset + b), (uint32_t)(step0 + k), break_half);
+    }
+}
+
+__global__ void k_discrete(const uint8_t* a, int B, float ld, int8_t* btn, float* look) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    int8_t b[8];
+    float l[2];
+    mc_discrete_to_buttons(a[i], ld, b, l);
+    for (int k = 0; k < 8; ++k) btn[(long long)i * 8 + k] = b[k];
+    look[(long long)i * 2 + 0] = l[0];
+    look[(long long)i * 2 + 1] = l[1];
+}
+
+inline int blocks(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+}  // namespace
+
+int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s) {
+    if (p->B == 0) return 0;
+    k_reset_masked<<<blocks(p->B, 256), 256, 0, s>>>(*p, mask);
+    return (int)cudaGetLastError();
+}
+
+int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s) {
+    int wxyz = p->wx * p->wy * p->wz;
+    int grid = p->B < 1184 ? (p->B > 0 ? p->B : 1) : 1184;  // 148 SMs x 8
+    k_regen<<<grid, 256, 0, s>>>(p->voxels, p->world_template, p->B, wxyz, p->flags, conditional);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// configuration
+// ---------------------------------------------------------------------------
+static int family_of(int obs_mode) {
+    switch (obs_mode) {
+        case MC_OBS_FLOAT32:
+        case MC_OBS_UINT8: return MC_FAM_SHADED;
+        case MC_OBS_UINT8_FAST: return MC_FAM_SHADED_FAST;
+        case MC_OBS_UINT8_MINIMAL: return MC_FAM_MINIMAL;
+        case MC_OBS_UINT8_FP16: return MC_FAM_FP16;
+        case MC_OBS_UINT8_PREBASIS:
+        case MC_OBS_UINT8_PREBASIS_FULL:
+        case MC_OBS_UINT8_SMEM: return MC_FAM_PREBASIS;
+        default: return -1;
+    }
+}
+
+static const mc_backend* backend_of(int numerics) {
+    if (numerics == MC_NUMERICS_REF_FAST) return mc_backend_fast();
+    if (numerics == MC_NUMERICS_IEEE) return mc_backend_ieee();
+    return nullptr;
+}
+
+static int check_config(const mc_env_config* c) {
+    if (!c) return fail(MC_ERR_INVALID, "config is NULL");
+    if (c->batch_size < 0) return fail(MC_ERR_INVALID, "batch_size %d < 0", c->batch_size);
+    if (c->world_x < 1 || c->world_y < 1 || c->world_z < 1)
+        return fail(MC_ERR_INVALID, "world dims must be >= 1 (got %d,%d,%d)", c->world_x, c->world_y, c->world_z);
+    long long wxyz = (long long)c->world_x * c->world_y * c->world_z;
+    if (wxyz > (1LL << 30)) return fail(MC_ERR_INVALID, "world too large (%lld voxels)", wxyz);
+    if (c->render_width < 1 || c->render_height < 1 || (long long)c->render_width * c->render_height > (1 << 24))
+        return fail(MC_ERR_INVALID, "render size %dx%d out of range", c->render_width, c->render_height);
+    if (family_of(c->obs_mode) < 0) return fail(MC_ERR_INVALID, "unknown obs_mode %d", c->obs_mode);
+    if (!backend_of(c->numerics)) return fail(MC_ERR_INVALID, "unknown numerics %d", c->numerics);
+    if (c->target_block < -128 || c->target_block > 127)
+        return fail(MC_ERR_INVALID, "target_block %d outside int8", c->target_block);
+    return MC_OK;
+}
+
+// MineEnv's spawn, tree and house positions (minecu/__init__.py:195-206).
+struct Placement {
+    float sx, sy, sz;
+    int tx, tz, hx, hz;
+};
+static Placement placement_of(const mc_env_config* c) {
+    Placement p;
+    p.sx = (float)(c->world_x / 2.0);
+    p.sy = (float)(c->ground_height + 2);
+    p.sz = (float)(c->world_z / 2.0);
+    if (c->spawn_override) {
+        p.sx = c->spawn_x;
+        p.sy = c->spawn_y;
+        p.sz = c->spawn_z;
+    }
+    p.tx = (int)(c->world_x / 2.0);
+    p.tz = (int)(c->world_z / 2.0) + 2;
+    p.hx = (int)(c->world_x / 2.0) + 6;
+    p.hz = (int)(c->world_z / 2.0) - 2;
+    return p;
+}
+
+static void fill_kp(mc_kp* k, const mc_env_config* c, const mc_env_state* s) {
+    memset(k, 0, sizeof(*k));
+    Placement pl = placement_of(c);
+    k->B = c->batch_size;
+    k->wx = c->world_x;
+    k->wy = c->world_y;
+    k->wz = c->world_z;
+    k->W = c->render_width;
+    k->H = c->render_height;
+    k->max_steps = c->max_steps;
+    k->vd = c->view_distance;
+    k->fov = c->fov_degrees;
+    k->dt = c->dt;
+    k->gravity = c->gravity;
+    k->walk_speed = c->walk_speed;
+    k->sprint_mult = c->sprint_mult;
+    k->jump_vel = c->jump_vel;
+    k->gh = c->ground_height;
+    k->target_block = c->target_block;
+    k->reward_value = c->reward_value;
+    k->spawn_x = pl.sx;
+    k->spawn_y = pl.sy;
+    k->spawn_z = pl.sz;
+    k->episode_rule = (c->obs_mode == MC_OBS_UINT8_PREBASIS_FULL) ? 1 : 0;
+    k->ext_done = 0;
+    k->has_limit = c->has_episode_limit;
+    k->episode_length = c->episode_length;
+    k->family = family_of(c->obs_mode);
+    k->obs_f32 = (c->obs_mode == MC_OBS_FLOAT32);
+    k->look_delta = c->look_delta;
+    if (s) {
+        k->voxels = s->voxels;
+        k->positions = s->positions;
+        k->velocities = s->velocities;
+        k->yaws = s->yaws;
+        k->pitches = s->pitches;
+        k->on_ground = s->on_ground;
+        k->step_count = s->step_count;
+        k->do_reset = s->do_reset;
+        k->cameras = s->cameras;
+        k->basis = s->basis;
+        k->obs = s->obs;
+        k->rewards = s->rewards;
+        k->dbg_interact = s->dbg_interact;
+        k->dbg_pixel = s->dbg_pixel;
+    }
+}
+
+static int check_state(const mc_env_config* c, const mc_env_state* s) {
+    if (!s) return fail(MC_ERR_INVALID, "state is NULL");
+    if (c->batch_size == 0) return MC_OK;
+    const void* req[] = {s->voxels, s->positions, s->velocities, s->yaws, s->pitches, s->on_ground,
+                         s->step_count, s->do_reset, s->cameras, s->obs, s->rewards};
+    const char* names[] = {"voxels", "positions", "velocities", "yaws", "pitches", "on_ground",
+                           "step_count", "do_reset", "cameras", "obs", "rewards"};
+    for (int i = 0; i < 11; ++i)
+        if (!req[i]) return fail(MC_ERR_INVALID, "state.%s is NULL", names[i]);
+    if (((uintptr_t)s->positions | (uintptr_t)s->velocities | (uintptr_t)s->yaws | (uintptr_t)s->pitches |
+         (uintptr_t)s->cameras | (uintptr_t)s->rewards | (uintptr_t)s->step_count) & 3)
+        return fail(MC_ERR_INVALID, "float/int32 state buffers must be 4-byte aligned");
+    if (family_of(c->obs_mode) == MC_FAM_PREBASIS && c->obs_mode != MC_OBS_UINT8_SMEM && !s->basis)
+        return fail(MC_ERR_INVALID, "prebasis modes need state.basis [B,14]");
+    return MC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// env handle
+// ---------------------------------------------------------------------------
+struct RolloutGraph {
+    cudaGraphExec_t exec = nullptr;
+    const uint8_t* actions = nullptr;
+    float* rewards_out = nullptr;
+    uint8_t* dones_out = nullptr;
+    int K = 0;
+    mc_fused_cfg fcfg{};
+    mc_kp kp{};
+};
+
+struct mc_env {
+    mc_env_config cfg;
+    mc_env_state st;
+    mc_kp kp;
+    const mc_backend* be;
+    int device;
+    int num_sms;
+    mc_fused_cfg fcfg;
+    int32_t* flags;
+    int8_t* tmpl;
+    uint8_t* scratch;  // plain-form decode buffers
+    cudaStream_t cap_stream;
+    std::vector<RolloutGraph> graphs;
+};
+
+static bool dones_possible(const mc_kp& k) {
+    if (k.ext_done) return false;
+    if (k.episode_rule == 0) return k.has_limit != 0;
+    return k.episode_length > 0;
+}
+
+static void default_fused(mc_env* e) {
+    // Staging a world in shared memory pays when it is small; the autotuner
+    // (minecu/autotune.py) refines this per configuration.
+    int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
+    e->fcfg.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
+    e->fcfg.warps_per_cta = 8;
+    e->fcfg.ctas_per_sm = 4;
+    e->fcfg.px_per_lane = 4;
+}
+
+static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
+    if (f->warps_per_cta != 4 && f->warps_per_cta != 8)
+        return fail(MC_ERR_INVALID, "warps_per_cta must be 4 or 8");
+    if (f->px_per_lane != 1 && f->px_per_lane != 2 && f->px_per_lane != 4)
+        return fail(MC_ERR_INVALID, "px_per_lane must be 1, 2 or 4");
+    if (f->ctas_per_sm < 1 || f->ctas_per_sm > 32) return fail(MC_ERR_INVALID, "ctas_per_sm out of range");
+    int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
+    if (f->stage && (wxyz & 15)) return fail(MC_ERR_INVALID, "stage needs world bytes %% 16 == 0");
+    mc_kp k = e->kp;
+    size_t smem = e->be->fused_smem_bytes(&k, f);
+    if (smem > 227 * 1024) return fail(MC_ERR_INVALID, "fused shared memory %zu > 227 KB", smem);
+    return MC_OK;
+}
+
+static void drop_graphs(mc_env* e) {
+    for (auto& g : e->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    e->graphs.clear();
+}
+
+extern "C" int mc_env_create(const mc_env_config* cfg, const mc_env_state* state, mc_env** out) {
+    if (!out) return fail(MC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    rc = check_state(cfg, state);
+    if (rc) return rc;
+    Placement pl = placement_of(cfg);
+    if (pl.tx < 0 || pl.tx >= cfg->world_x || pl.tz < 0 || pl.tz >= cfg->world_z)
+        return fail(MC_ERR_INVALID,
+                    "tree at (%d,%d) outside the %dx%d world (world_z must be >= 5); the reference writes out of "
+                    "bounds here",
+                    pl.tx, pl.tz, cfg->world_x, cfg->world_z);
+    mc_env* e = new mc_env();
+    e->cfg = *cfg;
+    e->st = *state;
+    e->be = backend_of(cfg->numerics);
+    fill_kp(&e->kp, cfg, state);
+    cudaError_t ce = cudaGetDevice(&e->device);
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device);
+    long long wxyz = (long long)cfg->world_x * cfg->world_y * cfg->world_z;
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->flags, MC_FLAG_WORDS * sizeof(int32_t));
+    if (ce == cudaSuccess) ce = cudaMemset(e->flags, 0, MC_FLAG_WORDS * sizeof(int32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->tmpl, (size_t)((wxyz + 15) & ~15LL));
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) {
+        // the template world: generate + tree + house on one env
+        k_generate_world<<<blocks((long long)cfg->world_y * cfg->world_x, 128), 128, 0, e->cap_stream>>>(
+            e->tmpl, (long long)cfg->world_y * cfg->world_x, cfg->world_x, cfg->world_y, cfg->world_z,
+            cfg->ground_height);
+        k_place_tree<<<1, 32, 0, e->cap_stream>>>(e->tmpl, 1, cfg->world_x, cfg->world_y, cfg->world_z, pl.tx, pl.tz,
+                                                   cfg->ground_height);
+        k_place_house<<<1, 32, 0, e->cap_stream>>>(e->tmpl, 1, cfg->world_x, cfg->world_y, cfg->world_z, pl.hx,
+                                                    pl.hz, cfg->ground_height);
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->cap_stream);
+    }
+    if (ce != cudaSuccess) {
+        int r = cuda_fail(ce, "mc_env_create");
+        mc_env_destroy(e);
+        return r;
+    }
+    e->kp.flags = e->flags;
+    e->kp.world_template = e->tmpl;
+    default_fused(e);
+    *out = e;
+    return MC_OK;
+}
+
+extern "C" int mc_env_destroy(mc_env* e) {
+    if (!e) return MC_OK;
+    drop_graphs(e);
+    if (e->flags) cudaFree(e->flags);
+    if (e->tmpl) cudaFree(e->tmpl);
+    if (e->scratch) cudaFree(e->scratch);
+    if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    delete e;
+    return MC_OK;
+}
+
+extern "C" int mc_env_set_state(mc_env* e, const mc_env_state* s) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    int rc = check_state(&e->cfg, s);
+    if (rc) return rc;
+    e->st = *s;
+    int32_t* flags = e->kp.flags;
+    const int8_t* tmpl = e->kp.world_template;
+    fill_kp(&e->kp, &e->cfg, s);
+    e->kp.flags = flags;
+    e->kp.world_template = tmpl;
+    drop_graphs(e);
+    return MC_OK;
+}
+
+static int ensure_scratch(mc_env* e) {
+    if (e->scratch || e->cfg.batch_size == 0) return MC_OK;
+    size_t B = (size_t)e->cfg.batch_size;
+    MC_CK(cudaMalloc(&e->scratch, B * (5 * 4 + 3) + 64));
+    uint8_t* p = e->scratch;
+    e->kp.s_fwd = (float*)p; p += B * 4;
+    e->kp.s_strafe = (float*)p; p += B * 4;
+    e->kp.s_dyaw = (float*)p; p += B * 4;
+    e->kp.s_dpitch = (float*)p; p += B * 4;
+    e->kp.s_speed = (float*)p; p += B * 4;
+    e->kp.s_jump = p; p += B;
+    e->kp.s_brk = p; p += B;
+    e->kp.s_place = p;
+    return MC_OK;
+}
+
+extern "C" int mc_env_generate_world(mc_env* e, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (e->cfg.batch_size == 0) return MC_OK;
+    return backend_rc(mc_launch_regen(&e->kp, 0, (cudaStream_t)stream), "regen");
+}
+
+static int render_obs(mc_env* e, cudaStream_t s) {
+    mc_kp k = e->kp;
+    if (k.B == 0) return MC_OK;
+    k_cameras_rt<<<blocks(k.B, 256), 256, 0, s>>>(k);
+    MC_CK(cudaGetLastError());
+    // MineEnv._render always uses the shaded kernel: float32 for "float32",
+    // render_uint8 for every uint8 mode (minecu/__init__.py:455-464).
+    return backend_rc(e->be->render(&k, MC_FAM_SHADED, s), "render");
+}
+
+extern "C" int mc_env_reset(mc_env* e, const uint8_t* mask, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (e->cfg.batch_size == 0) return MC_OK;
+    int rc = backend_rc(mc_launch_reset_agents(&e->kp, mask, s), "reset");
+    if (rc) return rc;
+    rc = backend_rc(mc_launch_regen(&e->kp, 1, s), "regen");
+    if (rc) return rc;
+    return render_obs(e, s);
+}
+
+static int do_step(mc_env* e, const int8_t* buttons, const float* look, const uint8_t* actions, int form,
+                   cudaStream_t s) {
+    if (e->cfg.batch_size == 0) return MC_OK;
+    mc_kp k = e->kp;
+    k.buttons = buttons;
+    k.look = look;
+    k.actions = actions;
+    int rc;
+    if (form == MC_FORM_PLAIN) {
+        rc = ensure_scratch(e);
+        if (rc) return rc;
+        k = e->kp;
+        k.buttons = buttons;
+        k.look = look;
+        k.actions = actions;
+        rc = backend_rc(e->be->step_plain(&k, s), "step_plain");
+    } else if (form == MC_FORM_FUSED) {
+        rc = backend_rc(e->be->step_fused(&k, &e->fcfg, e->num_sms, s), "step_fused");
+    } else {
+        return fail(MC_ERR_INVALID, "unknown form %d", form);
+    }
+    if (rc) return rc;
+    if (dones_possible(k)) return backend_rc(mc_launch_regen(&k, 1, s), "regen");
+    return MC_OK;
+}
+
+extern "C" int mc_env_step(mc_env* e, const int8_t* buttons, const float* look, int form, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (e->cfg.batch_size && (!buttons || !look)) return fail(MC_ERR_INVALID, "buttons/look are NULL");
+    if (((uintptr_t)look) & 3) return fail(MC_ERR_INVALID, "look must be 4-byte aligned");
+    return do_step(e, buttons, look, nullptr, form, (cudaStream_t)stream);
+}
+
+extern "C" int mc_env_step_discrete(mc_env* e, const uint8_t* actions, int form, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (e->cfg.batch_size && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    return do_step(e, nullptr, nullptr, actions, form, (cudaStream_t)stream);
+}
+
+extern "C" int mc_env_render(mc_env* e, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    return render_obs(e, (cudaStream_t)stream);
+}
+
+static bool same_fcfg(const mc_fused_cfg& a, const mc_fused_cfg& b) {
+    return a.stage == b.stage && a.warps_per_cta == b.warps_per_cta && a.ctas_per_sm == b.ctas_per_sm &&
+           a.px_per_lane == b.px_per_lane;
+}
+
+static int rollout_graph(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
+                         RolloutGraph** out) {
+    *out = nullptr;
+    RolloutGraph* hit = nullptr;
+    for (auto& g : e->graphs)
+        if (g.actions == actions && g.K == K && g.rewards_out == rewards_out && g.dones_out == dones_out &&
+            same_fcfg(g.fcfg, e->fcfg))
+            hit = &g;
+    if (!hit) {
+        // capture K fused steps (+ conditional regeneration and output copies)
+        long long B = e->cfg.batch_size;
+        cudaGraph_t graph = nullptr;
+        MC_CK(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int rc = MC_OK;
+        for (int k = 0; k < K && rc == MC_OK; ++k) {
+            rc = do_step(e, nullptr, nullptr, actions + (long long)k * B, MC_FORM_FUSED, e->cap_stream);
+            if (rc == MC_OK && rewards_out) {
+                cudaError_t ce = cudaMemcpyAsync(rewards_out + (long long)k * B, e->kp.rewards, B * sizeof(float),
+                                                 cudaMemcpyDeviceToDevice, e->cap_stream);
+                if (ce) rc = cuda_fail(ce, "rollout copy");
+            }
+            if (rc == MC_OK && dones_out) {
+                cudaError_t ce = cudaMemcpyAsync(dones_out + (long long)k * B, e->kp.do_reset, B,
+                                                 cudaMemcpyDeviceToDevice, e->cap_stream);
+                if (ce) rc = cuda_fail(ce, "rollout copy");
+            }
+        }
+        cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        RolloutGraph g;
+        ce = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+        g.actions = actions;
+        g.K = K;
+        g.rewards_out = rewards_out;
+        g.dones_out = dones_out;
+        g.fcfg = e->fcfg;
+        if (e->graphs.size() >= 8) {
+            cudaGraphExecDestroy(e->graphs.front().exec);
+            e->graphs.erase(e->graphs.begin());
+        }
+        e->graphs.push_back(g);
+        hit = &e->graphs.back();
+    }
+    *out = hit;
+    return MC_OK;
+}
+
+static int rollout_args(mc_env* e, const uint8_t* actions, int32_t K) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (K < 0) return fail(MC_ERR_INVALID, "K < 0");
+    if (K > 0 && e->cfg.batch_size > 0 && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    return MC_OK;
+}
+
+extern "C" int mc_env_rollout_prepare(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out,
+                                      uint8_t* dones_out) {
+    int rc = rollout_args(e, actions, K);
+    if (rc || K == 0 || e->cfg.batch_size == 0) return rc;
+    RolloutGraph* g;
+    return rollout_graph(e, actions, K, rewards_out, dones_out, &g);
+}
+
+extern "C" int mc_env_rollout(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
+                              void* stream) {
+    int rc = rollout_args(e, actions, K);
+    if (rc || K == 0 || e->cfg.batch_size == 0) return rc;
+    RolloutGraph* g;
+    rc = rollout_graph(e, actions, K, rewards_out, dones_out, &g);
+    if (rc) return rc;
+    MC_CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return MC_OK;
+}
+
+extern "C" int mc_env_set_fused_config(mc_env* e, const mc_fused_config* c) {
+    if (!e || !c) return fail(MC_ERR_INVALID, "NULL argument");
+    mc_fused_cfg f{c->stage, c->warps_per_cta, c->ctas_per_sm, c->px_per_lane};
+    int rc = validate_fused(e, &f);
+    if (rc) return rc;
+    e->fcfg = f;
+    return MC_OK;
+}
+
+extern "C" int mc_env_get_fused_config(const mc_env* e, mc_fused_config* c) {
+    if (!e || !c) return fail(MC_ERR_INVALID, "NULL argument");
+    c->stage = e->fcfg.stage;
+    c->warps_per_cta = e->fcfg.warps_per_cta;
+    c->ctas_per_sm = e->fcfg.ctas_per_sm;
+    c->px_per_lane = e->fcfg.px_per_lane;
+    return MC_OK;
+}
+
+extern "C" int64_t mc_env_fused_smem_bytes(const mc_env* e) {
+    if (!e) return -1;
+    mc_kp k = e->kp;
+    return (int64_t)e->be->fused_smem_bytes(&k, &e->fcfg);
+}
+
+extern "C" int mc_env_check_error(mc_env* e, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    int32_t h[MC_FLAG_WORDS];
+    cudaStream_t s = (cudaStream_t)stream;
+    MC_CK(cudaMemcpyAsync(h, e->flags, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MC_CK(cudaStreamSynchronize(s));
+    if (h[MC_FLAG_ERROR] != MC_KERR_NONE) {
+        int code = h[MC_FLAG_ERROR];
+        int32_t zero = 0;
+        MC_CK(cudaMemcpyAsync(e->flags + MC_FLAG_ERROR, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
+        MC_CK(cudaStreamSynchronize(s));
+        return fail(MC_ERR_KERNEL, "kernel error %d (%s)", code,
+                    code == MC_KERR_TMA_TIMEOUT ? "bulk copy wait timed out" : "unknown");
+    }
+    return MC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stateless entry points (the reference's _C functions)
+// ---------------------------------------------------------------------------
+static int32_t* stateless_flags() {
+    // one flag block per device for the stand-alone entry points; the any-done
+    // flag they set is never read (their callers regenerate from Python)
+    static int32_t* per_dev[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!per_dev[dev]) {
+        int32_t* p = nullptr;
+        if (cudaMalloc(&p, MC_FLAG_WORDS * sizeof(int32_t)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, MC_FLAG_WORDS * sizeof(int32_t));
+        per_dev[dev] = p;
+    }
+    return per_dev[dev];
+}
+
+extern "C" int mc_generate_world(int8_t* vox, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t gh, uint32_t seed,
+                                 void* stream) {
+    (void)seed;  // unused by the reference's generator too (kernels.cu:1800)
+    if (B < 0 || wx < 1 || wy < 1 || wz < 1) return fail(MC_ERR_INVALID, "bad world dims");
+    if (B == 0) return MC_OK;
+    if (!vox) return fail(MC_ERR_INVALID, "voxels is NULL");
+    long long rows = (long long)B * wy * wx;
+    k_generate_world<<<blocks(rows, 128), 128, 0, (cudaStream_t)stream>>>(vox, rows, wx, wy, wz, gh);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
+extern "C" int mc_place_tree(int8_t* vox, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t tx, int32_t tz,
+                             int32_t gh, void* stream) {
+    if (B < 0 || wx < 1 || wy < 1 || wz < 1) return fail(MC_ERR_INVALID, "bad world dims");
+    if (tx < 0 || tx >= wx || tz < 0 || tz >= wz)
+        return fail(MC_ERR_INVALID, "tree at (%d,%d) outside the world; the reference writes out of bounds here", tx,
+                    tz);
+    if (B == 0) return MC_OK;
+    if (!vox) return fail(MC_ERR_INVALID, "voxels is NULL");
+    k_place_tree<<<blocks(B, 256), 256, 0, (cudaStream_t)stream>>>(vox, B, wx, wy, wz, tx, tz, gh);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
+extern "C" int mc_place_house(int8_t* vox, int32_t B, int32_t wx, int32_t wy, int32_t wz, int32_t hx, int32_t hz,
+                              int32_t gh, void* stream) {
+    if (B < 0 || wx < 1 || wy < 1 || wz < 1) return fail(MC_ERR_INVALID, "bad world dims");
+    if (B == 0) return MC_OK;
+    if (!vox) return fail(MC_ERR_INVALID, "voxels is NULL");
+    k_place_house<<<blocks(B, 256), 256, 0, (cudaStream_t)stream>>>(vox, B, wx, wy, wz, hx, hz, gh);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
+extern "C" int mc_reset_agents(float* pos, float* vel, float* yaw, float* pitch, uint8_t* og, const uint8_t* dr,
+                               int32_t B, float sx, float sy, float sz, void* stream) {
+    if (B < 0) return fail(MC_ERR_INVALID, "B < 0");
+    if (B == 0) return MC_OK;
+    if (!pos || !vel || !yaw || !pitch || !og || !dr) return fail(MC_ERR_INVALID, "NULL buffer");
+    k_reset_agents<<<blocks(B, 256), 256, 0, (cudaStream_t)stream>>>(pos, vel, yaw, pitch, og, dr, B, sx, sy, sz);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
+extern "C" int mc_render(const mc_env_config* cfg, const mc_env_state* st, int32_t shaded, void* stream) {
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    if (!st || (cfg->batch_size && (!st->voxels || !st->obs))) return fail(MC_ERR_INVALID, "NULL buffer");
+    mc_kp k;
+    fill_kp(&k, cfg, st);
+    int fam = shaded ? (cfg->obs_mode == MC_OBS_UINT8_FAST ? MC_FAM_SHADED_FAST : MC_FAM_SHADED) : k.family;
+    if (fam == MC_FAM_PREBASIS ? !st->basis : !st->cameras) return fail(MC_ERR_INVALID, "cameras/basis is NULL");
+    return backend_rc(backend_of(cfg->numerics)->render(&k, fam, (cudaStream_t)stream), "render");
+}
+
+extern "C" int mc_precompute_camera_basis(const float* cameras, float* basis, int32_t B, int32_t W, int32_t H,
+                                          float fov, int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics");
+    if (B < 0 || W < 1 || H < 1) return fail(MC_ERR_INVALID, "bad sizes");
+    if (B == 0) return MC_OK;
+    if (!cameras || !basis) return fail(MC_ERR_INVALID, "NULL buffer");
+    mc_kp k;
+    memset(&k, 0, sizeof(k));
+    k.B = B;
+    k.W = W;
+    k.H = H;
+    k.fov = fov;
+    k.cameras = (float*)cameras;
+    k.basis = basis;
+    return backend_rc(be->basis(&k, (cudaStream_t)stream), "basis");
+}
+
+extern "C" int mc_render_uint8_prebasis(const int8_t* vox, const float* basis, uint8_t* out, int32_t B, int32_t wx,
+                                        int32_t wy, int32_t wz, int32_t W, int32_t H, int32_t max_steps,
+                                        int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics");
+    if (B < 0 || W < 1 || H < 1 || wx < 1 || wy < 1 || wz < 1) return fail(MC_ERR_INVALID, "bad sizes");
+    if (B == 0) return MC_OK;
+    if (!vox || !basis || !out) return fail(MC_ERR_INVALID, "NULL buffer");
+    mc_kp k;
+    memset(&k, 0, sizeof(k));
+    k.B = B;
+    k.wx = wx;
+    k.wy = wy;
+    k.wz = wz;
+    k.W = W;
+    k.H = H;
+    k.max_steps = max_steps;
+    k.voxels = (int8_t*)vox;
+    k.basis = (float*)basis;
+    k.obs = out;
+    k.family = MC_FAM_PREBASIS;
+    return backend_rc(be->render(&k, MC_FAM_PREBASIS, (cudaStream_t)stream), "render_prebasis");
+}
+
+extern "C" int mc_render_uint8_coalesced(const int8_t* vox, const float* basis, uint8_t* out, int32_t B, int32_t ws,
+                                         int32_t W, int32_t H, int32_t max_steps, int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics");
+    if (B < 0 || W < 1 || H < 1 || ws < 1) return fail(MC_ERR_INVALID, "bad sizes");
+    if (B == 0) return MC_OK;
+    if (!vox || !basis || !out) return fail(MC_ERR_INVALID, "NULL buffer");
+    return backend_rc(be->render_coalesced(vox, basis, out, B, ws, W, H, max_steps, (cudaStream_t)stream),
+                      "render_coalesced");
+}
+
+extern "C" int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* st, const int8_t* buttons,
+                                 const float* look, const mc_decode_buffers* dec, int32_t form, void* stream) {
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    rc = check_state(cfg, st);
+    if (rc) return rc;
+    if (cfg->batch_size == 0) return MC_OK;
+    if (!buttons || !look) return fail(MC_ERR_INVALID, "buttons/look are NULL");
+    mc_kp k;
+    fill_kp(&k, cfg, st);
+    k.ext_done = (cfg->obs_mode == MC_OBS_UINT8_PREBASIS_FULL) ? 0 : 1;
+    k.buttons = buttons;
+    k.look = look;
+    k.flags = stateless_flags();
+    if (!k.flags) return fail(MC_ERR_CUDA, "flag buffer allocation failed");
+    const mc_backend* be = backend_of(cfg->numerics);
+    if (form == MC_FORM_PLAIN) {
+        if (!dec || !dec->forward_in || !dec->strafe_in || !dec->delta_yaw_in || !dec->delta_pitch_in ||
+            !dec->jump_in || !dec->do_break || !dec->do_place || !dec->speed_mult)
+            return fail(MC_ERR_INVALID, "the plain form needs the 8 decode buffers");
+        k.s_fwd = dec->forward_in;
+        k.s_strafe = dec->strafe_in;
+        k.s_dyaw = dec->delta_yaw_in;
+        k.s_dpitch = dec->delta_pitch_in;
+        k.s_jump = dec->jump_in;
+        k.s_brk = dec->do_break;
+        k.s_place = dec->do_place;
+        k.s_speed = dec->speed_mult;
+        return backend_rc(be->step_plain(&k, (cudaStream_t)stream), "step_plain");
+    }
+    if (form == MC_FORM_FUSED) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        mc_fused_cfg f;
+        int wxyz = cfg->world_x * cfg->world_y * cfg->world_z;
+        f.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
+        f.warps_per_cta = 8;
+        f.ctas_per_sm = 4;
+        f.px_per_lane = 4;
+        return backend_rc(be->step_fused(&k, &f, sms, (cudaStream_t)stream), "step_fused");
+    }
+    return fail(MC_ERR_INVALID, "unknown form %d", form);
+}
+
+extern "C" int mc_physics(float* pos, float* vel, float* yaw, float* pitch, uint8_t* og, const float* fwd,
+                          const float* strafe, const float* dyaw, const float* dpitch, const uint8_t* jump,
+                          const float* speed, int32_t B, int32_t ws, float dt, float gravity, float walk_speed,
+                          float jump_vel, int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics");
+    if (B < 0 || ws < 1) return fail(MC_ERR_INVALID, "bad sizes");
+    if (B == 0) return MC_OK;
+    mc_kp k;
+    memset(&k, 0, sizeof(k));
+    k.B = B;
+    k.wx = k.wy = k.wz = ws;  // cubic, as launch_physics (kernels.cu:2244-2249)
+    k.dt = dt;
+    k.gravity = gravity;
+    k.walk_speed = walk_speed;
+    k.jump_vel = jump_vel;
+    k.positions = pos;
+    k.velocities = vel;
+    k.yaws = yaw;
+    k.pitches = pitch;
+    k.on_ground = og;
+    k.s_fwd = (float*)fwd;
+    k.s_strafe = (float*)strafe;
+    k.s_dyaw = (float*)dyaw;
+    k.s_dpitch = (float*)dpitch;
+    k.s_jump = (uint8_t*)jump;
+    k.s_speed = (float*)speed;
+    // physics reads brk/place only through load_dec; point them at jump (unused)
+    k.s_brk = (uint8_t*)jump;
+    k.s_place = (uint8_t*)jump;
+    return backend_rc(be->physics(&k, (cudaStream_t)stream), "physics");
+}
+
+extern "C" int mc_raycast_break(int8_t* vox, const float* pos, const float* yaw, const float* pitch,
+                                const uint8_t* do_break, float* rewards, int32_t B, int32_t ws, int32_t target_block,
+                                float reward_value, int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics");
+    if (B < 0 || ws < 1) return fail(MC_ERR_INVALID, "bad sizes");
+    if (target_block < -128 || target_block > 127) return fail(MC_ERR_INVALID, "target_block outside int8");
+    if (B == 0) return MC_OK;
+    mc_kp k;
+    memset(&k, 0, sizeof(k));
+    k.B = B;
+    k.wx = k.wy = k.wz = ws;
+    k.voxels = vox;
+    k.positions = (float*)pos;
+    k.yaws = (float*)yaw;
+    k.pitches = (float*)pitch;
+    k.s_brk = (uint8_t*)do_break;
+    k.s_place = (uint8_t*)do_break;
+    k.rewards = rewards;
+    k.target_block = target_block;
+    k.reward_value = reward_value;
+    // load_agent reads velocities and on_ground; the break kernel only uses
+    // position and view, so point those reads at valid memory
+    k.velocities = (float*)pos;
+    k.on_ground = (uint8_t*)do_break;
+    return backend_rc(be->interact(&k, 1, (cudaStream_t)stream), "raycast_break");
+}
+
+extern "C" int mc_philox_actions(uint8_t* actions, int32_t B, int32_t K, int32_t env_offset, int32_t step0,
+                                 uint64_t seed, int32_t break_half, void* stream) {
+    if (B < 0 || K < 0) return fail(MC_ERR_INVALID, "bad sizes");
+    long long n = (long long)B * K;
+    if (n == 0) return MC_OK;
+    if (!actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    int grid = (int)((n + 255) / 256);
+    if (grid > 148 * 32) grid = 148 * 32;
+    k_philox<<<grid, 256, 0, (cudaStream_t)stream>>>(actions, B, K, env_offset, step0, seed, break_half);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
+extern "C" int mc_discrete_to_buttons(const uint8_t* actions, int32_t B, float look_delta, int8_t* buttons,
+                                      float* look, void* stream) {
+    if (B < 0) return fail(MC_ERR_INVALID, "B < 0");
+    if (B == 0) return MC_OK;
+    if (!actions || !buttons || !look) return fail(MC_ERR_INVALID, "NULL buffer");
+    k_discrete<<<blocks(B, 256), 256, 0, (cudaStream_t)stream>>>(actions, B, look_delta, buttons, look);
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}

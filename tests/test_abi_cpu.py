@@ -1,0 +1,67 @@
+"""The C-ABI library loads, exports every function include/minecu_b200.h
+declares, and rejects bad arguments on the host (no GPU needed)."""
+import ctypes
+
+import pytest
+
+from minecu import capi
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    names = capi.header_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert L.mc_abi_version() == 1
+
+
+def test_prototypes_cover_header():
+    assert set(capi.header_functions()) == set(capi._PROTOS)
+
+
+def _cfg(**kw):
+    base = dict(batch_size=4, world_x=16, world_y=16, world_z=16, render_width=8, render_height=8)
+    base.update(kw)
+    return capi.make_config(**base)
+
+
+@pytest.mark.parametrize("bad", [dict(batch_size=-1), dict(world_x=0), dict(render_width=0),
+                                 dict(target_block=300), dict(world_z=4)])
+def test_env_create_rejects_bad_config(bad):
+    L = capi.lib()
+    c = _cfg(**bad)
+    st = capi.EnvState()
+    for f, _ in capi.EnvState._fields_:
+        setattr(st, f, 16)  # never dereferenced: validation fails first
+    h = ctypes.c_void_p()
+    rc = L.mc_env_create(ctypes.byref(c), ctypes.byref(st), ctypes.byref(h))
+    assert rc == capi.MC_ERR_INVALID, capi.last_error()
+    assert capi.last_error()
+    assert not h.value
+
+
+def test_bad_enums_and_null_state():
+    L = capi.lib()
+    c = _cfg()
+    c.obs_mode = 42
+    st = capi.EnvState()
+    h = ctypes.c_void_p()
+    assert L.mc_env_create(ctypes.byref(c), ctypes.byref(st), ctypes.byref(h)) == capi.MC_ERR_INVALID
+    c = _cfg()
+    c.numerics = 9
+    assert L.mc_env_create(ctypes.byref(c), ctypes.byref(st), ctypes.byref(h)) == capi.MC_ERR_INVALID
+    c = _cfg()
+    assert L.mc_env_create(ctypes.byref(c), ctypes.byref(st), ctypes.byref(h)) == capi.MC_ERR_INVALID
+    assert "NULL" in capi.last_error()
+
+
+def test_stateless_entry_points_validate_before_launch():
+    L = capi.lib()
+    assert L.mc_place_tree(None, 1, 8, 8, 8, 9, 2, 4, None) == capi.MC_ERR_INVALID  # tree outside
+    assert L.mc_generate_world(None, 1, 0, 8, 8, 4, 0, None) == capi.MC_ERR_INVALID
+    assert L.mc_precompute_camera_basis(None, None, 1, 8, 8, 70.0, 7, None) == capi.MC_ERR_INVALID
+    assert L.mc_philox_actions(None, -1, 1, 0, 0, 0, 0, None) == capi.MC_ERR_INVALID
+    # zero-sized work is a no-op, not an error
+    assert L.mc_generate_world(None, 0, 8, 8, 8, 4, 0, None) == capi.MC_OK
+    assert L.mc_env_destroy(None) == capi.MC_OK
