@@ -175,93 +175,104 @@ def run_mine(args):
     if args.launch:
         st, wpc, cps, ppl = (int(x) for x in args.launch.split(","))
         env.set_launch_config(st, wpc, cps, ppl)
-    env.reset()
     stream = torch.cuda.current_stream()
-    acts_w = torch.empty((max(Wm, 1), B), dtype=torch.uint8, device=dev)
+    # every arm below replays steps [0, Wm) untimed and [Wm, Wm+K) timed of
+    # the same seeded trajectory, starting from reset()
+    acts_w = torch.empty((Wm, B), dtype=torch.uint8, device=dev)
     acts_t = torch.empty((K, B), dtype=torch.uint8, device=dev)
     _C.philox_actions(acts_w, rank * B, 0, W["seed"])
     _C.philox_actions(acts_t, rank * B, Wm, W["seed"])
     env.prepare_rollout(acts_w)
     env.prepare_rollout(acts_t)
     torch.cuda.synchronize()
-
-    # ---- fused step in a CUDA graph (value) --------------------------------
-    env.rollout(acts_w[:Wm] if Wm else acts_w[:0])
-    torch.cuda.synchronize()
-    barrier(world)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+
+    def timed(fn):
         torch.cuda.synchronize()
+        barrier(world)
         ev0.record(stream)
-        env.rollout(acts_t)
+        fn()
         ev1.record(stream)
         torch.cuda.synchronize()
-    barrier(world)
-    t_fused = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+        barrier(world)
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+
+    # ---- fused step, K steps in one CUDA graph (value) ----------------------
+    env.reset()
+    env.rollout(acts_w)
+    with ClockSampler(local) as clk:
+        t_fused = timed(lambda: env.rollout(acts_t))
     env.check_error()
     value = B * K * world / t_fused
-    ms_step = t_fused / K * 1e3
+
+    # ---- same, L2 flushed (a 256 MB write) before every step ----------------
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    env.reset()
+    env.rollout(acts_w)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    for s in range(K):
+        flush.fill_(s & 255)
+        starts[s].record(stream)
+        _C.env_step_discrete(env._env, acts_t[s], 1)
+        ends[s].record(stream)
+    torch.cuda.synchronize()
+    t_flushed = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / 1e3, world)
+    del flush
 
     # ---- plain form (the reference's kernel sequence, eager) ---------------
-    Kp = min(K, args.plain_steps)
     env.form = "plain"
-    for s in range(min(Wm, 5)):
-        env.step(acts_w[s % acts_w.shape[0]])
-    torch.cuda.synchronize()
-    barrier(world)
-    ev0.record(stream)
-    for s in range(Kp):
-        env.step(acts_t[s])
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
-    plain_value = B * Kp * world / t_plain
+    env.reset()
+    for s in range(Wm):
+        env.step(acts_w[s])
+    t_plain = timed(lambda: [env.step(acts_t[s]) for s in range(K)])
+    plain_value = B * K * world / t_plain
     env.form = "fused"
 
     # ---- e2e through the public API with host buffers ------------------------
-    Ke = min(K, args.e2e_steps)
-    h_acts = acts_t[:Ke].cpu().pin_memory()
-    h_rew = torch.empty((Ke, B), dtype=torch.float32).pin_memory()
-    h_done = torch.empty((Ke, B), dtype=torch.bool).pin_memory()
+    h_acts = torch.cat([acts_w, acts_t]).cpu().pin_memory()
+    h_rew = torch.empty((K, B), dtype=torch.float32).pin_memory()
+    h_done = torch.empty((K, B), dtype=torch.bool).pin_memory()
     d_act = torch.empty((B,), dtype=torch.uint8, device=dev)
-    for s in range(min(Wm, 5)):
+    env.reset()
+    for s in range(Wm):
         d_act.copy_(h_acts[s], non_blocking=True)
         env.step(d_act)
-    torch.cuda.synchronize()
-    barrier(world)
-    ev0.record(stream)
-    for s in range(Ke):
-        d_act.copy_(h_acts[s], non_blocking=True)
-        obs, rew, done = env.step(d_act)
-        h_rew[s].copy_(rew, non_blocking=True)
-        h_done[s].copy_(done, non_blocking=True)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t_e2e = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
-    e2e_value = B * Ke * world / t_e2e
+
+    def e2e_loop():
+        for s in range(K):
+            d_act.copy_(h_acts[Wm + s], non_blocking=True)
+            obs, rew, done = env.step(d_act)
+            h_rew[s].copy_(rew, non_blocking=True)
+            h_done[s].copy_(done, non_blocking=True)
+
+    t_e2e = timed(e2e_loop)
+    e2e_value = B * K * world / t_e2e
     _ = float(h_rew.sum())  # the host reads the results
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_ENV_STEP * B / (t_fused / K) / 1e9
-    traffic = None
-    if args.traffic_bytes:
-        traffic = float(args.traffic_bytes)
     line = {
         "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": K, "warmup": Wm,
-        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": t_fused / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
         "config": {"workload": W["workload"], "global_batch": B * world, "world": "16x16x16",
                    "render": "32x32x3 uint8", "obs_dtype": W["obs_dtype"], "numerics": "ref_fast",
                    "form": "fused persistent kernel, K-step CUDA graph", "launch": env.launch_config(),
                    "parallelism": f"env-sharded x{world} (no collective)",
-                   "l2": "per-step working set 235 MB (worlds 134 MB + obs 101 MB) > 126 MB L2; no flush"},
-        "plain": {"value": plain_value, "unit": "env-steps/s", "steps": Kp,
-                  "ms_per_step": t_plain / Kp * 1e3, "fused_speedup": value / plain_value},
-        "e2e": {"value": e2e_value, "unit": "env-steps/s", "steps": Ke, "h2d_bytes_per_step": B,
+                   "trajectory": f"steps {Wm}..{Wm + K - 1} after reset(), every arm",
+                   "l2": "per-step working set 235 MB (worlds 134 MB + obs 101 MB) > 126 MB L2; no flush "
+                         "(l2_flushed: 256 MB write before every step)"},
+        "l2_flushed": {"value": B * K * world / t_flushed, "unit": "env-steps/s",
+                       "ms_per_step": t_flushed / K * 1e3},
+        "plain": {"value": plain_value, "unit": "env-steps/s", "ms_per_step": t_plain / K * 1e3,
+                  "fused_speedup": value / plain_value},
+        "e2e": {"value": e2e_value, "unit": "env-steps/s", "h2d_bytes_per_step": B,
                 "d2h_bytes_per_step": B * 4 + B,
                 "path": "MineEnv.step(actions) per step; pinned H2D actions, D2H rewards+dones"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic": float(args.traffic_bytes) if args.traffic_bytes else None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_env_step": BYTES_PER_ENV_STEP,
                      "kernel": "k_step_fused (avg over the timed region)"},
         "gpu_launches": K,
@@ -296,8 +307,7 @@ def run_reference(args):
     dev = torch.device("cuda", local)
     env = ref_driver.RefEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
                             device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], target_block=3)
-    env.reset()
-    Kr = min(K, args.ref_steps)
+    Kr = K
     btns = torch.empty((Kr + Wm, B, 8), dtype=torch.int8)
     looks = torch.empty((Kr + Wm, B, 2), dtype=torch.float32)
     for s in range(Kr + Wm):
@@ -305,6 +315,7 @@ def run_reference(args):
         btns[s] = torch.from_numpy(b)
         looks[s] = torch.from_numpy(l)
     d_btn, d_look = btns.to(dev), looks.to(dev)
+    env.reset()
     for s in range(Wm):
         env.step(d_btn[s], d_look[s])
     torch.cuda.synchronize()
@@ -321,6 +332,9 @@ def run_reference(args):
     h_btn, h_look = btns.pin_memory(), looks.pin_memory()
     h_rew = torch.empty((Kr, B), dtype=torch.float32).pin_memory()
     h_done = torch.empty((Kr, B), dtype=torch.bool).pin_memory()
+    env.reset()
+    for s in range(Wm):
+        env.step(d_btn[s], d_look[s])
     torch.cuda.synchronize()
     ev0.record(stream)
     for s in range(Kr):
@@ -336,6 +350,7 @@ def run_reference(args):
         "warmup": Wm, "ms_per_step": t / Kr * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
         "config": {"workload": W["workload"], "global_batch": B, "obs_dtype": W["obs_dtype"],
+                   "trajectory": f"steps {Wm}..{Wm + Kr - 1} after reset()",
                    "path": "reference src/kernels.cu launch_step_uint8 + MineEnv.step glue (eager, default stream)"},
         "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": B * 16, "d2h_bytes_per_step": B * 5},
         "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": None, "kind": "reference",
@@ -351,9 +366,6 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--plain-steps", type=int, default=200)
-    ap.add_argument("--e2e-steps", type=int, default=500)
-    ap.add_argument("--ref-steps", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,px_per_lane")

@@ -46,8 +46,24 @@ __constant__ uint8_t c_sky8[3] = {135, 206, 235};
 // ---------------------------------------------------------------------------
 // Numerics policy
 // ---------------------------------------------------------------------------
+// Arithmetic is written with explicit single-rounding ops so that the
+// compiler cannot contract or reorder it differently in different contexts
+// (kernel shape, basic blocks, hoisting):
+//   mul/add/sub  one IEEE rounding each (never fused);
+//   mad(a,b,c)   ref_fast: one fused multiply-add, exactly where the
+//                reference build's compiler fuses (determined by comparing
+//                outputs with the reference's kernels on millions of inputs);
+//                ieee: a*b rounded, then + c rounded (the CPU checker's order).
 #if MC_NUMERICS_FAST
 struct N {
+    static __device__ __forceinline__ float mad(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    // a/b - 1 and 1 - a/b: the build turns the division into a*(1/b) with an
+    // approximate reciprocal and fuses it with the +-1
+    static __device__ __forceinline__ float div_sub1(float a, float b) { return __fmaf_rn(a, __fdividef(1.0f, b), -1.0f); }
+    static __device__ __forceinline__ float one_sub_div(float a, float b) { return __fmaf_rn(-a, __fdividef(1.0f, b), 1.0f); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return cosf(x); }
     static __device__ __forceinline__ float tan(float x) { return tanf(x); }
@@ -58,6 +74,12 @@ struct N {
 };
 #else
 struct N {
+    static __device__ __forceinline__ float mad(float a, float b, float c) { return __fadd_rn(__fmul_rn(a, b), c); }
+    static __device__ __forceinline__ float div_sub1(float a, float b) { return __fsub_rn(__fdiv_rn(a, b), 1.0f); }
+    static __device__ __forceinline__ float one_sub_div(float a, float b) { return __fsub_rn(1.0f, __fdiv_rn(a, b)); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
     static __device__ __forceinline__ float sin(float x) { return mc_ieee_sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return mc_ieee_cosf(x); }
     static __device__ __forceinline__ float tan(float x) { return mc_ieee_tanf(x); }
@@ -79,8 +101,8 @@ struct Dec {
 // decode_actions_kernel (kernels.cu:1459-1504)
 __device__ __forceinline__ Dec decode_buttons(const int8_t b[8], float l0, float l1, float sprint_mult) {
     Dec d;
-    d.fwd = (float)b[0] - (float)b[1];
-    d.strafe = (float)b[3] - (float)b[2];
+    d.fwd = N::sub((float)b[0], (float)b[1]);
+    d.strafe = N::sub((float)b[3], (float)b[2]);
     d.dyaw = l0;
     d.dpitch = l1;
     d.jump = (b[4] != 0);
@@ -137,22 +159,27 @@ __device__ __forceinline__ void store_agent(const mc_kp& p, long long i, const A
 
 // physics_kernel (kernels.cu:1511-1584): rotate, walk, gravity, clamp to the
 // flat ground at world_y/4 and to [1, W-1] in x and z.  No voxel collision.
+//   move_x = ((sin*fwd)*speed)*dt + ((cos*str)*walk)*dt   (the build fuses the strafe product)
+//   move_z = ((cos*fwd)*speed)*dt - ((sin*str)*walk)*dt   (the build fuses the forward product)
+//   vel_y += gravity*dt;  y += vel_y*dt                   (both fused)
 __device__ __forceinline__ void physics(Agent& a, const Dec& d, const mc_kp& p) {
-    a.yaw = a.yaw + d.dyaw;
-    float new_pitch = a.pitch + d.dpitch;
+    a.yaw = N::add(a.yaw, d.dyaw);
+    float new_pitch = N::add(a.pitch, d.dpitch);
     a.pitch = fminf(fmaxf(new_pitch, -1.56f), 1.56f);
     float cos_yaw = N::cos(a.yaw);
     float sin_yaw = N::sin(a.yaw);
     float fwd = d.fwd, str = d.strafe;
-    float speed = p.walk_speed * d.speed;
-    float move_x = sin_yaw * fwd * speed * p.dt + cos_yaw * str * p.walk_speed * p.dt;
-    float move_z = cos_yaw * fwd * speed * p.dt - sin_yaw * str * p.walk_speed * p.dt;
+    float speed = N::mul(p.walk_speed, d.speed);
+    float fx_ = N::mul(N::mul(N::mul(sin_yaw, fwd), speed), p.dt);
+    float move_x = N::mad(N::mul(N::mul(cos_yaw, str), p.walk_speed), p.dt, fx_);
+    float sz_ = N::mul(N::mul(N::mul(sin_yaw, str), p.walk_speed), p.dt);
+    float move_z = N::mad(N::mul(N::mul(cos_yaw, fwd), speed), p.dt, -sz_);
     float vel_y = a.vy;
     if (d.jump && a.og) vel_y = p.jump_vel;
-    vel_y += p.gravity * p.dt;
-    float new_x = a.x + move_x;
-    float new_y = a.y + vel_y * p.dt;
-    float new_z = a.z + move_z;
+    vel_y = N::mad(p.gravity, p.dt, vel_y);
+    float new_x = N::add(a.x, move_x);
+    float new_y = N::mad(vel_y, p.dt, a.y);
+    float new_z = N::add(a.z, move_z);
     float ground_y = (float)(p.wy / 4);
     if (new_y <= ground_y) {
         new_y = ground_y;
@@ -162,8 +189,8 @@ __device__ __forceinline__ void physics(Agent& a, const Dec& d, const mc_kp& p) 
         a.og = false;
     }
     float margin = 1.0f;
-    new_x = fminf(fmaxf(new_x, margin), (float)p.wx - margin);
-    new_z = fminf(fmaxf(new_z, margin), (float)p.wz - margin);
+    new_x = fminf(fmaxf(new_x, margin), N::sub((float)p.wx, margin));
+    new_z = fminf(fmaxf(new_z, margin), N::sub((float)p.wz, margin));
     a.x = new_x;
     a.y = new_y;
     a.z = new_z;
@@ -200,10 +227,10 @@ __device__ __forceinline__ Sample interact_sample(int k, float eye_x, float eye_
                                                   float dir_x, float dir_y, float dir_z,
                                                   int wx, int wy, int wz) {
     float reach = 4.0f;
-    float t = 0.1f + k * (reach / 32.0f);
-    float px = eye_x + dir_x * t;
-    float py = eye_y + dir_y * t;
-    float pz = eye_z + dir_z * t;
+    float t = N::mad((float)k, reach / 32.0f, 0.1f);  // k/8 is exact: same value fused or not
+    float px = N::mad(dir_x, t, eye_x);
+    float py = N::mad(dir_y, t, eye_y);
+    float pz = N::mad(dir_z, t, eye_z);
     int vx = (int)floorf(px);
     int vy = (int)floorf(py);
     int vz = (int)floorf(pz);
@@ -218,9 +245,9 @@ __device__ __forceinline__ void interact_dir(const Agent& a, float& dx, float& d
     float sin_yaw = N::sin(a.yaw);
     float cos_pitch = N::cos(a.pitch);
     float sin_pitch = N::sin(a.pitch);
-    dx = sin_yaw * cos_pitch;
+    dx = N::mul(sin_yaw, cos_pitch);
     dy = sin_pitch;
-    dz = cos_yaw * cos_pitch;
+    dz = N::mul(cos_yaw, cos_pitch);
 }
 
 __device__ __forceinline__ bool reward_hit(const mc_kp& p, int8_t blk) {
@@ -236,7 +263,7 @@ __device__ __forceinline__ int interact_seq(int8_t* w, const Agent& a, bool brk,
     if (!brk && !place) return -1;
     float dx, dy, dz;
     interact_dir(a, dx, dy, dz);
-    float eye_x = a.x, eye_y = a.y + 1.6f, eye_z = a.z;
+    float eye_x = a.x, eye_y = N::add(a.y, 1.6f), eye_z = a.z;
     int prev = -1;
     for (int k = 0; k < 32; ++k) {
         Sample s = interact_sample(k, eye_x, eye_y, eye_z, dx, dy, dz, p.wx, p.wy, p.wz);
@@ -272,7 +299,7 @@ __device__ __forceinline__ int interact_warp(int8_t* w, const Agent& a, bool brk
     if (!brk && !place) return -1;  // warp-uniform
     float dx, dy, dz;
     interact_dir(a, dx, dy, dz);
-    Sample s = interact_sample(lane, a.x, a.y + 1.6f, a.z, dx, dy, dz, p.wx, p.wy, p.wz);
+    Sample s = interact_sample(lane, a.x, N::add(a.y, 1.6f), a.z, dx, dy, dz, p.wx, p.wy, p.wz);
     int8_t blk = s.inb ? w[s.idx] : AIR;
     unsigned solid = __ballot_sync(0xffffffffu, s.inb && blk >= 0);
     unsigned inbm = __ballot_sync(0xffffffffu, s.inb);
@@ -300,7 +327,8 @@ __device__ __forceinline__ int interact_warp(int8_t* w, const Agent& a, bool brk
 // ---------------------------------------------------------------------------
 struct Cam {
     float eye_x, eye_y, eye_z;
-    float fx, fy, fz, rx, rz, ux, uy, uz;
+    float fx, fy, fz, rx, rz, ux, uy, uz;  // forward, right (x, z), up
+    float sy, cy, cp;                      // sin/cos yaw, cos pitch (TRIG ray pattern)
 };
 
 // Camera basis as the per-pixel code of render_kernel / _uint8 / _minimal /
@@ -310,22 +338,45 @@ struct Cam {
 __device__ __forceinline__ Cam cam_trig(float cx, float cy, float cz, float yaw, float pitch) {
     Cam c;
     c.eye_x = cx;
-    c.eye_y = cy + 1.6f;
+    c.eye_y = N::add(cy, 1.6f);
     c.eye_z = cz;
     float cos_yaw = N::cos(yaw);
     float sin_yaw = N::sin(yaw);
     float cos_pitch = N::cos(pitch);
     float sin_pitch = N::sin(pitch);
-    c.fx = sin_yaw * cos_pitch;
+    c.fx = N::mul(sin_yaw, cos_pitch);
     c.fy = sin_pitch;
-    c.fz = cos_yaw * cos_pitch;
+    c.fz = N::mul(cos_yaw, cos_pitch);
     c.rx = cos_yaw;
     c.rz = -sin_yaw;
-    c.ux = -sin_yaw * sin_pitch;
+    c.ux = N::mul(-sin_yaw, sin_pitch);
     c.uy = cos_pitch;
-    c.uz = -cos_yaw * sin_pitch;
+    c.uz = N::mul(-cos_yaw, sin_pitch);
+    c.sy = sin_yaw;
+    c.cy = cos_yaw;
+    c.cp = cos_pitch;
     return c;
 }
+
+// Ray direction before normalisation, forward + u*right + v*up.  Where the
+// reference computes the basis in the same kernel (TRIG: shaded, minimal,
+// fp16) its compiler fuses the forward product: fma(v, up, fma(sin, cos,
+// u*right)); where the basis is loaded (prebasis) it fuses u*right:
+// fma(v, up, fma(u, right, forward)).
+template <bool TRIG>
+__device__ __forceinline__ void ray_dir(const Cam& c, float u, float v, float& x, float& y, float& z) {
+    if (TRIG) {
+        x = N::mad(v, c.ux, N::mad(c.sy, c.cp, N::mul(u, c.rx)));
+        z = N::mad(v, c.uz, N::mad(c.cy, c.cp, N::mul(u, c.rz)));
+    } else {
+        x = N::mad(v, c.ux, N::mad(u, c.rx, c.fx));
+        z = N::mad(v, c.uz, N::mad(u, c.rz, c.fz));
+    }
+    y = N::mad(v, c.uy, c.fy);
+}
+
+// |ray|^2 = fma(z, z, fma(y, y, x*x))
+__device__ __forceinline__ float len2(float x, float y, float z) { return N::mad(z, z, N::mad(y, y, N::mul(x, x))); }
 
 // precompute_camera_basis_kernel (kernels.cu:511-561), all 13 written words.
 __device__ __forceinline__ void basis_compute(float cx, float cy, float cz, float yaw, float pitch,
@@ -333,31 +384,31 @@ __device__ __forceinline__ void basis_compute(float cx, float cy, float cz, floa
     float sin_yaw, cos_yaw, sin_pitch, cos_pitch;
     N::sincos_i(yaw, &sin_yaw, &cos_yaw);
     N::sincos_i(pitch, &sin_pitch, &cos_pitch);
-    float fov_rad = fov * 0.01745329f;
-    float half_fov = N::tan(fov_rad * 0.5f);
+    float fov_rad = N::mul(fov, 0.01745329f);
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
     float aspect = N::div((float)width, (float)height);
     out[0] = cx;
-    out[1] = cy + 1.6f;
+    out[1] = N::add(cy, 1.6f);
     out[2] = cz;
-    out[3] = sin_yaw * cos_pitch;
+    out[3] = N::mul(sin_yaw, cos_pitch);
     out[4] = sin_pitch;
-    out[5] = cos_yaw * cos_pitch;
+    out[5] = N::mul(cos_yaw, cos_pitch);
     out[6] = cos_yaw;
     out[7] = -sin_yaw;
-    out[8] = -sin_yaw * sin_pitch;
+    out[8] = N::mul(-sin_yaw, sin_pitch);
     out[9] = cos_pitch;
-    out[10] = -cos_yaw * sin_pitch;
-    out[11] = half_fov * aspect;
+    out[10] = N::mul(-cos_yaw, sin_pitch);
+    out[11] = N::mul(half_fov, aspect);
     out[12] = half_fov;
 }
 
 // scale_u / scale_v of precompute_camera_basis_kernel (kernels.cu:541-559);
 // they do not depend on the camera.
 __device__ __forceinline__ void prebasis_scales(int width, int height, float fov, float* su, float* sv) {
-    float fov_rad = fov * 0.01745329f;
-    float half_fov = N::tan(fov_rad * 0.5f);
+    float fov_rad = N::mul(fov, 0.01745329f);
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
     float aspect = N::div((float)width, (float)height);
-    *su = half_fov * aspect;
+    *su = N::mul(half_fov, aspect);
     *sv = half_fov;
 }
 
@@ -367,6 +418,7 @@ __device__ __forceinline__ Cam cam_from_basis(const float* b) {
     c.fx = b[3]; c.fy = b[4]; c.fz = b[5];
     c.rx = b[6]; c.rz = b[7];
     c.ux = b[8]; c.uy = b[9]; c.uz = b[10];
+    c.sy = 0.0f; c.cy = 0.0f; c.cp = 0.0f;  // unused by the prebasis ray pattern
     return c;
 }
 
@@ -374,34 +426,36 @@ __device__ __forceinline__ Cam cam_from_basis(const float* b) {
 // coordinate and launch constants, so the fused kernel tabulates them.
 // Shaded family: kernels.cu:129-134 (fov_rad = fov * 3.14159265 / 180).
 __device__ __forceinline__ float u_shaded(int px, int width, int height, float fov) {
-    float fov_rad = fov * 3.14159265f / 180.0f;
+    float fov_rad = N::div(N::mul(fov, 3.14159265f), 180.0f);
     float aspect = N::div((float)width, (float)height);
-    float half_fov = N::tan(fov_rad * 0.5f);
-    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * half_fov * aspect;
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
+    float a = N::div_sub1(N::mul(2.0f, N::add((float)px, 0.5f)), (float)width);
+    return N::mul(N::mul(a, half_fov), aspect);
 }
 __device__ __forceinline__ float v_shaded(int py, int height, float fov) {
-    float fov_rad = fov * 3.14159265f / 180.0f;
-    float half_fov = N::tan(fov_rad * 0.5f);
-    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * half_fov;
+    float fov_rad = N::div(N::mul(fov, 3.14159265f), 180.0f);
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
+    return N::mul(N::one_sub_div(N::mul(2.0f, N::add((float)py, 0.5f)), (float)height), half_fov);
 }
 // Minimal/fp16 family: kernels.cu:1029-1034 (fov_rad = fov * 0.01745329).
 __device__ __forceinline__ float u_minimal(int px, int width, int height, float fov) {
-    float fov_rad = fov * 0.01745329f;
+    float fov_rad = N::mul(fov, 0.01745329f);
     float aspect = N::div((float)width, (float)height);
-    float half_fov = N::tan(fov_rad * 0.5f);
-    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * half_fov * aspect;
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
+    float a = N::div_sub1(N::mul(2.0f, N::add((float)px, 0.5f)), (float)width);
+    return N::mul(N::mul(a, half_fov), aspect);
 }
 __device__ __forceinline__ float v_minimal(int py, int height, float fov) {
-    float fov_rad = fov * 0.01745329f;
-    float half_fov = N::tan(fov_rad * 0.5f);
-    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * half_fov;
+    float fov_rad = N::mul(fov, 0.01745329f);
+    float half_fov = N::tan(N::mul(fov_rad, 0.5f));
+    return N::mul(N::one_sub_div(N::mul(2.0f, N::add((float)py, 0.5f)), (float)height), half_fov);
 }
 // Prebasis family: kernels.cu:616-617 (scales from the basis).
 __device__ __forceinline__ float u_prebasis(int px, int width, float scale_u) {
-    return (N::div(2.0f * (px + 0.5f), (float)width) - 1.0f) * scale_u;
+    return N::mul(N::div_sub1(N::mul(2.0f, N::add((float)px, 0.5f)), (float)width), scale_u);
 }
 __device__ __forceinline__ float v_prebasis(int py, int height, float scale_v) {
-    return (1.0f - N::div(2.0f * (py + 0.5f), (float)height)) * scale_v;
+    return N::mul(N::one_sub_div(N::mul(2.0f, N::add((float)py, 0.5f)), (float)height), scale_v);
 }
 
 // Voxel sources for the ray march.
@@ -429,9 +483,9 @@ struct Hit {
 // given the precomputed numerators (0 - eye) and (ws - eye).
 __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float lo_x, float hi_x,
                                            float lo_y, float hi_y, float lo_z, float hi_z, float* t_entry) {
-    float t1 = lo_x * ix, t2 = hi_x * ix;
-    float t3 = lo_y * iy, t4 = hi_y * iy;
-    float t5 = lo_z * iz, t6 = hi_z * iz;
+    float t1 = N::mul(lo_x, ix), t2 = N::mul(hi_x, ix);
+    float t3 = N::mul(lo_y, iy), t4 = N::mul(hi_y, iy);
+    float t5 = N::mul(lo_z, iz), t6 = N::mul(hi_z, iz);
     *t_entry = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
     return fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
 }
@@ -447,10 +501,9 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 template <bool FASTG, class V>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
                                          int max_steps, float vd, int gh, bool inside) {
-    float ray_x = c.fx + u * c.rx + v * c.ux;
-    float ray_y = c.fy + v * c.uy;
-    float ray_z = c.fz + u * c.rz + v * c.uz;
-    float ray_len = N::sqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
+    float ray_x, ray_y, ray_z;
+    ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
+    float ray_len = N::sqrt(len2(ray_x, ray_y, ray_z));
     ray_x = N::div(ray_x, ray_len);
     ray_y = N::div(ray_y, ray_len);
     ray_z = N::div(ray_z, ray_len);
@@ -458,9 +511,9 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V
     float ix = (ray_x != 0.0f) ? N::div(1.0f, ray_x) : 1e30f;
     float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
     float iz = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 1e30f;
-    float lo_x = 0.0f - c.eye_x, hi_x = (float)wx - c.eye_x;
-    float lo_y = 0.0f - c.eye_y, hi_y = (float)wy - c.eye_y;
-    float lo_z = 0.0f - c.eye_z, hi_z = (float)wz - c.eye_z;
+    float lo_x = N::sub(0.0f, c.eye_x), hi_x = N::sub((float)wx, c.eye_x);
+    float lo_y = N::sub(0.0f, c.eye_y), hi_y = N::sub((float)wy, c.eye_y);
+    float lo_z = N::sub(0.0f, c.eye_z), hi_z = N::sub((float)wz, c.eye_z);
 
     Hit h;
     h.step_y = (ray_y >= 0) ? 1 : -1;
@@ -482,9 +535,9 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V
     int sy = h.step_y;
     int sz = (ray_z >= 0) ? 1 : -1;
     float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
-    float tmx = (ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ix : ((float)vx - c.eye_x) * ix;
-    float tmy = (ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iy : ((float)vy - c.eye_y) * iy;
-    float tmz = (ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * iz : ((float)vz - c.eye_z) * iz;
+    float tmx = N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ix);
+    float tmy = N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iy);
+    float tmz = N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), iz);
     float t = 0.0f;
     int face = -1;
     int wxz = wx * wz;
@@ -509,11 +562,11 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V
             if (t > t_exit) break;
         }
         if (tmx < tmy && tmx < tmz) {
-            t = tmx; tmx += tdx; vx += sx; face = 0;
+            t = tmx; tmx = N::add(tmx, tdx); vx += sx; face = 0;
         } else if (tmy < tmz) {
-            t = tmy; tmy += tdy; vy += sy; face = 1;
+            t = tmy; tmy = N::add(tmy, tdy); vy += sy; face = 1;
         } else {
-            t = tmz; tmz += tdz; vz += sz; face = 2;
+            t = tmz; tmz = N::add(tmz, tdz); vz += sz; face = 2;
         }
     }
     h.face = face;
@@ -526,7 +579,20 @@ __device__ __forceinline__ bool eye_inside(const Cam& c, int wx, int wy, int wz,
            c.eye_z > 0.0f && c.eye_z < (float)wz && vd >= 0.0f;
 }
 
+// Which product each channel's c*shade*(1-fog) + sky*fog fuses in the
+// reference build (measured against its kernels): float32 render_kernel
+// fuses sky*fog for red only; render_kernel_uint8 for red and green;
+// render_kernel_uint8_fast for red only (MC_FASTG_SKY).  Bit k = channel k.
+enum { MC_COL_F32 = 0, MC_COL_U8 = 1, MC_COL_U8FAST = 2 };
+#ifndef MC_FASTG_SKY
+#define MC_FASTG_SKY 0x1
+#endif
+__device__ __forceinline__ int sky_fused_mask(int kind) {
+    return kind == MC_COL_F32 ? 0x1 : (kind == MC_COL_U8 ? 0x3 : MC_FASTG_SKY);
+}
+
 // Shading and fog of the shaded family (kernels.cu:271-292, 446-469).
+template <int KIND>
 __device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*rgb)[3], const float* sky, float out[3]) {
     if (h.blk >= 0) {
         float r = rgb[h.blk][0], g = rgb[h.blk][1], b_col = rgb[h.blk][2];
@@ -535,10 +601,15 @@ __device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*
         else if (h.face == 2) shade = 0.9f;
         else if (h.face == 1 && h.step_y < 0) shade = 0.6f;
         float fog = fminf(N::div(h.t, vd), 1.0f);
-        fog = fog * fog;
-        out[0] = r * shade * (1.0f - fog) + sky[0] * fog;
-        out[1] = g * shade * (1.0f - fog) + sky[1] * fog;
-        out[2] = b_col * shade * (1.0f - fog) + sky[2] * fog;
+        fog = N::mul(fog, fog);
+        float omf = N::sub(1.0f, fog);
+        const int m = sky_fused_mask(KIND);
+        const float c3[3] = {r, g, b_col};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float cs = N::mul(c3[k], shade);
+            out[k] = ((m >> k) & 1) ? N::mad(sky[k], fog, N::mul(cs, omf)) : N::mad(cs, omf, N::mul(sky[k], fog));
+        }
     } else {
         out[0] = sky[0];
         out[1] = sky[1];
@@ -546,21 +617,20 @@ __device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*
     }
 }
 
-__device__ __forceinline__ uint32_t to_u8(float x) { return (uint32_t)(uint8_t)(x * 255.0f); }
+__device__ __forceinline__ uint32_t to_u8(float x) { return (uint32_t)(uint8_t)N::mul(x, 255.0f); }
 
 // Flat ray of render_kernel_uint8_minimal / _prebasis / _smem
 // (kernels.cu:1036-1097, 619-679): rsqrtf normalisation, no AABB, no fog,
 // unsigned bounds test, non-cubic world.
-template <class V>
+template <bool TRIG, class V>
 __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
                                         int max_steps) {
-    float ray_x = c.fx + u * c.rx + v * c.ux;
-    float ray_y = c.fy + v * c.uy;
-    float ray_z = c.fz + u * c.rz + v * c.uz;
-    float ray_len = N::rsqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
-    ray_x *= ray_len;
-    ray_y *= ray_len;
-    ray_z *= ray_len;
+    float ray_x, ray_y, ray_z;
+    ray_dir<TRIG>(c, u, v, ray_x, ray_y, ray_z);
+    float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
+    ray_x = N::mul(ray_x, ray_len);
+    ray_y = N::mul(ray_y, ray_len);
+    ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
     int vx = (int)floorf(c.eye_x);
     int vy = (int)floorf(c.eye_y);
@@ -572,9 +642,9 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
     float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
     float iz = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 1e30f;
     float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
-    float tmx = (ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ix : ((float)vx - c.eye_x) * ix;
-    float tmy = (ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iy : ((float)vy - c.eye_y) * iy;
-    float tmz = (ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * iz : ((float)vz - c.eye_z) * iz;
+    float tmx = N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ix);
+    float tmy = N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iy);
+    float tmz = N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), iz);
     Hit h;
     h.blk = AIR;
     h.face = -1;
@@ -590,11 +660,11 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
             }
         }
         if (tmx < tmy && tmx < tmz) {
-            tmx += tdx; vx += sx; face = 0;
+            tmx = N::add(tmx, tdx); vx += sx; face = 0;
         } else if (tmy < tmz) {
-            tmy += tdy; vy += sy; face = 1;
+            tmy = N::add(tmy, tdy); vy += sy; face = 1;
         } else {
-            tmz += tdz; vz += sz; face = 2;
+            tmz = N::add(tmz, tdz); vz += sz; face = 2;
         }
     }
     h.face = face;
@@ -606,13 +676,12 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
 template <class V>
 __device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
                                         int max_steps) {
-    float ray_x = c.fx + u * c.rx + v * c.ux;
-    float ray_y = c.fy + v * c.uy;
-    float ray_z = c.fz + u * c.rz + v * c.uz;
-    float ray_len = N::rsqrt(ray_x * ray_x + ray_y * ray_y + ray_z * ray_z);
-    ray_x *= ray_len;
-    ray_y *= ray_len;
-    ray_z *= ray_len;
+    float ray_x, ray_y, ray_z;
+    ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
+    float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
+    ray_x = N::mul(ray_x, ray_len);
+    ray_y = N::mul(ray_y, ray_len);
+    ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
     int vx = (int)floorf(c.eye_x);
     int vy = (int)floorf(c.eye_y);
@@ -626,9 +695,9 @@ __device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V&
     __half tdx = __float2half(fabsf(ixf));
     __half tdy = __float2half(fabsf(iyf));
     __half tdz = __float2half(fabsf(izf));
-    __half tmx = __float2half((ray_x >= 0) ? ((float)(vx + 1) - c.eye_x) * ixf : ((float)vx - c.eye_x) * ixf);
-    __half tmy = __float2half((ray_y >= 0) ? ((float)(vy + 1) - c.eye_y) * iyf : ((float)vy - c.eye_y) * iyf);
-    __half tmz = __float2half((ray_z >= 0) ? ((float)(vz + 1) - c.eye_z) * izf : ((float)vz - c.eye_z) * izf);
+    __half tmx = __float2half(N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ixf));
+    __half tmy = __float2half(N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iyf));
+    __half tmz = __float2half(N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), izf));
     Hit h;
     h.blk = AIR;
     h.face = -1;
@@ -788,7 +857,7 @@ __global__ void __launch_bounds__(128) k_render_shaded(mc_kp p) {
     VoxLdg vox{p.voxels + b * (long long)p.wx * p.wy * p.wz};
     Hit h = shade_ray<FASTG>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
     float rgb[3];
-    shade_rgb(h, p.vd, c_rgb, c_sky, rgb);
+    shade_rgb<F32 ? MC_COL_F32 : (FASTG ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, c_rgb, c_sky, rgb);
     if (F32) {
         float* o = (float*)p.obs + idx * 3;
         o[0] = rgb[0]; o[1] = rgb[1]; o[2] = rgb[2];
@@ -799,23 +868,17 @@ __global__ void __launch_bounds__(128) k_render_shaded(mc_kp p) {
     if (p.dbg_pixel) p.dbg_pixel[idx] = dbg_code(h);
 }
 
-// Flat render (minimal / fp16: 1-D grid over pixels with per-pixel trig;
-// prebasis: 2-D grid (pixel blocks, env) reading the [B,14] basis).
+// Flat render, one thread per pixel over B*H*W (minimal / fp16: per-pixel
+// trig; prebasis: reads the [B,14] basis).  The reference launches the
+// prebasis kernel on a 2-D grid (pixel blocks, env), which caps B at 65535;
+// the per-pixel work is the same.
 template <int FAM>
 __global__ void __launch_bounds__(128) k_render_flat(mc_kp p) {
-    long long b;
-    int pix;
     long long hw = (long long)p.H * p.W;
-    if (FAM == MC_FAM_PREBASIS) {
-        b = blockIdx.y;
-        pix = blockIdx.x * blockDim.x + threadIdx.x;
-        if (pix >= hw) return;
-    } else {
-        long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (idx >= (long long)p.B * hw) return;
-        b = idx / hw;
-        pix = (int)(idx - b * hw);
-    }
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)p.B * hw) return;
+    long long b = idx / hw;
+    int pix = (int)(idx - b * hw);
     int py = pix / p.W, px = pix - py * p.W;
     Cam c;
     float u, v;
@@ -837,7 +900,8 @@ __global__ void __launch_bounds__(128) k_render_flat(mc_kp p) {
     VoxLdg vox{p.voxels + b * wxyz};
     Hit h;
     if (FAM == MC_FAM_FP16) h = fp16_ray(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
-    else h = flat_ray(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    else if (FAM == MC_FAM_PREBASIS) h = flat_ray<false>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    else h = flat_ray<true>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     long long o = (b * hw + pix);
     uint8_t* out = (uint8_t*)p.obs + o * 3;
     const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
@@ -867,7 +931,7 @@ __global__ void __launch_bounds__(128) k_render_coalesced(const int8_t* vox, con
             return __ldg(v + (long long)idx * B + b);
         }
     } acc{vox, B, b, ws};
-    Hit h = flat_ray(c, u, v, acc, ws, ws, ws, max_steps);
+    Hit h = flat_ray<false>(c, u, v, acc, ws, ws, ws, max_steps);
     const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
     uint8_t* o = out + ((long long)b * H * W + pix) * 3;
     o[0] = col[0]; o[1] = col[1]; o[2] = col[2];
@@ -933,8 +997,17 @@ __device__ __forceinline__ void fill_pattern16(uint8_t* dst, int bytes, uint4 p0
     }
 }
 
+// Next env for this warp: claimed from a device counter (dynamic schedule,
+// balances the uneven per-env work) or by static striding.
+__device__ __forceinline__ long long next_env(const mc_kp& p, long long cur, long long total_warps, int lane) {
+    if (!p.sched_dynamic) return cur + total_warps;
+    unsigned v = 0;
+    if (lane == 0) v = atomicAdd(reinterpret_cast<unsigned*>(&p.flags[MC_FLAG_WORK]), 1u);
+    return (long long)__shfl_sync(0xffffffffu, v, 0);
+}
+
 template <int FAM, bool F32, bool STAGE, int PPL>
-__global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
+__global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -987,8 +1060,9 @@ __global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
     bool failed = false;
 
     const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
-    for (long long e = (long long)blockIdx.x * nwarps + warp; e < p.B && !failed;
-         e += (long long)gridDim.x * nwarps) {
+    const long long total_warps = (long long)gridDim.x * nwarps;
+    const long long first = p.sched_dynamic ? next_env(p, 0, total_warps, lane) : (long long)blockIdx.x * nwarps + warp;
+    for (long long e = first; e < p.B && !failed; e = next_env(p, e, total_warps, lane)) {
         // ---- agent step (every lane computes the same values) --------------
         int8_t btn[8];
         float l0, l1;
@@ -1066,7 +1140,8 @@ __global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
             uint8_t bytes[12];
             if (F32 || FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                 float rgb[3];
-                shade_rgb(h, p.vd, s_rgb, s_sky, rgb);
+                shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, s_rgb,
+                                                                                                      s_sky, rgb);
                 if (F32) {
                     // pattern period 12 bytes
 #pragma unroll
@@ -1151,13 +1226,15 @@ __global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
                         if (STAGE) h = fp16_ray(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                         else h = fp16_ray(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     } else {
-                        if (STAGE) h = flat_ray(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
-                        else h = flat_ray(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        constexpr bool TRIG = (FAM != MC_FAM_PREBASIS);
+                        if (STAGE) h = flat_ray<TRIG>(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        else h = flat_ray<TRIG>(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     }
                     const int so = (j * 32 + lane);
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         float rgb[3];
-                        shade_rgb(h, p.vd, s_rgb, s_sky, rgb);
+                        shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
+                            h, p.vd, s_rgb, s_sky, rgb);
                         if (F32) {
                             float* sf = reinterpret_cast<float*>(stage) + so * 3;
                             sf[0] = rgb[0]; sf[1] = rgb[1]; sf[2] = rgb[2];
@@ -1190,7 +1267,21 @@ __global__ void __launch_bounds__(256) k_step_fused(mc_kp p) {
             __syncwarp();
         }
     }
-    if (__syncthreads_or(any_done ? 1 : 0) && threadIdx.x == 0) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
+    // No CTA barrier here: warps leave as soon as their last env is done.
+    if (lane == 0) {
+        if (any_done) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
+        if (p.sched_dynamic) {
+            // every claim of this warp has returned (the last one >= B); the
+            // last warp to get here resets the counters for the next launch
+            __threadfence();
+            unsigned prev = atomicAdd(reinterpret_cast<unsigned*>(&p.flags[MC_FLAG_WARPS_DONE]), 1u);
+            if (prev == (unsigned)(total_warps - 1)) {
+                p.flags[MC_FLAG_WORK] = 0;
+                p.flags[MC_FLAG_WARPS_DONE] = 0;
+                __threadfence();
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1215,11 +1306,9 @@ static int render_launch(const mc_kp* p, int family, cudaStream_t s) {
         case MC_FAM_FP16:
             k_render_flat<MC_FAM_FP16><<<grid_1d(total, 128), 128, 0, s>>>(*p);
             break;
-        case MC_FAM_PREBASIS: {
-            dim3 g(grid_1d((long long)p->H * p->W, 128), p->B);
-            k_render_flat<MC_FAM_PREBASIS><<<g, 128, 0, s>>>(*p);
+        case MC_FAM_PREBASIS:
+            k_render_flat<MC_FAM_PREBASIS><<<grid_1d(total, 128), 128, 0, s>>>(*p);
             break;
-        }
         default:
             return (int)cudaErrorInvalidValue;
     }

@@ -14,7 +14,14 @@ enum {
 };
 
 // Device flag words owned by an env handle.
-enum { MC_FLAG_ANY_DONE = 0, MC_FLAG_REGEN_CTR = 1, MC_FLAG_ERROR = 2, MC_FLAG_WORDS = 8 };
+enum {
+    MC_FLAG_ANY_DONE = 0,    // set by a step when any env is done
+    MC_FLAG_REGEN_CTR = 1,   // CTAs of the regeneration kernel that finished
+    MC_FLAG_ERROR = 2,       // MC_KERR_* recorded by a kernel
+    MC_FLAG_WORK = 3,        // next env to claim (fused kernel, dynamic schedule)
+    MC_FLAG_WARPS_DONE = 4,  // warps of the fused kernel that finished
+    MC_FLAG_WORDS = 8
+};
 
 // Error codes a kernel can record in flags[MC_FLAG_ERROR] (never a trap).
 enum { MC_KERR_NONE = 0, MC_KERR_TMA_TIMEOUT = 1 };
@@ -33,6 +40,8 @@ struct mc_kp {
     int episode_rule;  // 0: python rule (has_limit && cnt >= L); 1: kernel rule (L > 0 && cnt >= L)
     int ext_done;      // 1: do_reset is an input and step_count is not touched (the reference's
                        //    _C.step* entry points, whose episode logic runs in Python)
+    int sched_dynamic; // fused kernel: 1 = warps claim envs from flags[MC_FLAG_WORK] (needs a
+                       // flag block no other launch uses concurrently); 0 = static striding
     int has_limit, episode_length;
     int family;   // MC_FAM_*
     int obs_f32;  // float32 obs (else uint8)

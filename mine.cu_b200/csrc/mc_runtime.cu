@@ -480,6 +480,7 @@ extern "C" int mc_env_create(const mc_env_config* cfg, const mc_env_state* state
     }
     e->kp.flags = e->flags;
     e->kp.world_template = e->tmpl;
+    e->kp.sched_dynamic = 1;  // the handle's flag block is used by one launch at a time
     default_fused(e);
     *out = e;
     return MC_OK;
@@ -506,6 +507,7 @@ extern "C" int mc_env_set_state(mc_env* e, const mc_env_state* s) {
     fill_kp(&e->kp, &e->cfg, s);
     e->kp.flags = flags;
     e->kp.world_template = tmpl;
+    e->kp.sched_dynamic = 1;
     drop_graphs(e);
     return MC_OK;
 }

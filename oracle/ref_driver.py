@@ -53,6 +53,10 @@ _PROTOS = {
     "launch_render_uint8_fast": [P, P, P, I, I, I, I, I, F, F, I],
     "launch_precompute_camera_basis": [P, P, I, I, I, F],
     "launch_render_uint8_prebasis": [P, P, P, I, I, I, I, I],
+    "launch_render_uint8_coalesced": [P, P, P, I, I, I, I, I],
+    "launch_physics": [P, P, P, P, P, P, P, P, P, P, P, I, I, F, F, F, F],
+    "launch_raycast_break": [P, P, P, P, P, P, I, I, I8, F],
+    "launch_decode_actions": [P, P, P, P, P, P, P, P, P, P, I, F],
 }
 
 _lib = None
