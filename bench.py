@@ -368,7 +368,7 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,px_per_lane")
+    ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,tile_w")
     ap.add_argument("--traffic-bytes", type=float, default=0.0,
                     help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

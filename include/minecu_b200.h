@@ -113,7 +113,7 @@ typedef struct mc_fused_config {
     int32_t stage;         /* 1: bulk-copy each marched world into shared memory */
     int32_t warps_per_cta; /* 4 or 8 */
     int32_t ctas_per_sm;   /* persistent grid = SMs x ctas_per_sm */
-    int32_t px_per_lane;   /* 1, 2 or 4 pixels per lane per chunk */
+    int32_t tile_w;        /* a warp marches tiles of tile_w x (32/tile_w) pixels: 4, 8, 16 or 32 */
 } mc_fused_config;
 
 /* ---- library ---------------------------------------------------------- */

@@ -64,6 +64,10 @@ struct N {
     static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
     static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
     static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    // a / b as the build computes it (a times the approximate reciprocal of
+    // b), with the reciprocal passed in so repeated divisors share it
+    static __device__ __forceinline__ float rcp_of(float b) { return __fdividef(1.0f, b); }
+    static __device__ __forceinline__ float div_r(float a, float b, float rcp_b) { (void)b; return __fmul_rn(a, rcp_b); }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return cosf(x); }
     static __device__ __forceinline__ float tan(float x) { return tanf(x); }
@@ -80,6 +84,8 @@ struct N {
     static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
     static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
     static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float rcp_of(float b) { (void)b; return 0.0f; }
+    static __device__ __forceinline__ float div_r(float a, float b, float rcp_b) { (void)rcp_b; return __fdiv_rn(a, b); }
     static __device__ __forceinline__ float sin(float x) { return mc_ieee_sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return mc_ieee_cosf(x); }
     static __device__ __forceinline__ float tan(float x) { return mc_ieee_tanf(x); }
@@ -331,6 +337,26 @@ struct Cam {
     float sy, cy, cp;                      // sin/cos yaw, cos pitch (TRIG ray pattern)
 };
 
+// Per-env constants of the DDA set-up: the eye's voxel and, per axis, the
+// distance numerators to its upper and lower faces, (v+1) - eye and v - eye.
+struct Dda0 {
+    int vx, vy, vz;
+    float nxp, nxm, nyp, nym, nzp, nzm;
+};
+__device__ __forceinline__ Dda0 dda0(const Cam& c) {
+    Dda0 d;
+    d.vx = (int)floorf(c.eye_x);
+    d.vy = (int)floorf(c.eye_y);
+    d.vz = (int)floorf(c.eye_z);
+    d.nxp = N::sub((float)(d.vx + 1), c.eye_x);
+    d.nxm = N::sub((float)d.vx, c.eye_x);
+    d.nyp = N::sub((float)(d.vy + 1), c.eye_y);
+    d.nym = N::sub((float)d.vy, c.eye_y);
+    d.nzp = N::sub((float)(d.vz + 1), c.eye_z);
+    d.nzm = N::sub((float)d.vz, c.eye_z);
+    return d;
+}
+
 // Camera basis as the per-pixel code of render_kernel / _uint8 / _minimal /
 // _fp16 / _fast computes it (kernels.cu:113-136): cosf/sinf of yaw/pitch.
 // Pure function of the camera, so computing it once per env gives the bits
@@ -498,15 +524,21 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // strictly inside the box and view_distance >= 0;
 // then the AABB test always passes (t_entry < 0 <= view_distance) and its
 // exit distance is only computed if the march leaves the world.
+// With `skip_first` (a per-env fact: the eye is inside the world, its voxel
+// holds air, view_distance > 0 and max_steps >= 1, and for FASTG the eye is
+// at or above the ground) the first loop iteration is known to advance
+// without a hit, so its tests are skipped.
 template <bool FASTG, class V>
-__device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
-                                         int max_steps, float vd, int gh, bool inside) {
+__device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
+                                         int wz, int max_steps, float vd, int gh, bool inside,
+                                         bool skip_first = false) {
     float ray_x, ray_y, ray_z;
     ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::sqrt(len2(ray_x, ray_y, ray_z));
-    ray_x = N::div(ray_x, ray_len);
-    ray_y = N::div(ray_y, ray_len);
-    ray_z = N::div(ray_z, ray_len);
+    const float rl = N::rcp_of(ray_len);
+    ray_x = N::div_r(ray_x, ray_len, rl);
+    ray_y = N::div_r(ray_y, ray_len, rl);
+    ray_z = N::div_r(ray_z, ray_len, rl);
 
     float ix = (ray_x != 0.0f) ? N::div(1.0f, ray_x) : 1e30f;
     float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
@@ -528,27 +560,39 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V
         have_exit = true;
         if (t_exit < 0 || t_entry > t_exit || t_entry > vd) return h;  // sky
     }
-    int vx = (int)floorf(c.eye_x);
-    int vy = (int)floorf(c.eye_y);
-    int vz = (int)floorf(c.eye_z);
+    int vx = d0.vx, vy = d0.vy, vz = d0.vz;
     int sx = (ray_x >= 0) ? 1 : -1;
     int sy = h.step_y;
     int sz = (ray_z >= 0) ? 1 : -1;
     float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
-    float tmx = N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ix);
-    float tmy = N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iy);
-    float tmz = N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), iz);
+    float tmx = N::mul((ray_x >= 0) ? d0.nxp : d0.nxm, ix);
+    float tmy = N::mul((ray_y >= 0) ? d0.nyp : d0.nym, iy);
+    float tmz = N::mul((ray_z >= 0) ? d0.nzp : d0.nzm, iz);
     float t = 0.0f;
     int face = -1;
-    int wxz = wx * wz;
-    for (int step = 0; step < max_steps; ++step) {
+    const int wxz = wx * wz;
+    // linear voxel index kept in step with (vx, vy, vz)
+    int idx = vy * wxz + vx * wz + vz;
+    const int dix = sx * wz, diy = sy * wxz, diz = sz;
+    int step = 0;
+    if (skip_first) {
+        if (tmx < tmy && tmx < tmz) {
+            t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0;
+        } else if (tmy < tmz) {
+            t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1;
+        } else {
+            t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2;
+        }
+        step = 1;
+    }
+    for (; step < max_steps; ++step) {
         if (t >= vd) break;
         if (FASTG && vy < gh) {
             h.blk = (vy == gh - 1) ? GRASS : DIRT;
             break;
         }
         if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
-            int8_t b = vox(vy * wxz + vx * wz + vz);
+            int8_t b = vox(idx);
             if (b >= 0) {
                 h.blk = b;
                 break;
@@ -562,11 +606,11 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, float u, float v, const V
             if (t > t_exit) break;
         }
         if (tmx < tmy && tmx < tmz) {
-            t = tmx; tmx = N::add(tmx, tdx); vx += sx; face = 0;
+            t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0;
         } else if (tmy < tmz) {
-            t = tmy; tmy = N::add(tmy, tdy); vy += sy; face = 1;
+            t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1;
         } else {
-            t = tmz; tmz = N::add(tmz, tdz); vz += sz; face = 2;
+            t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2;
         }
     }
     h.face = face;
@@ -593,14 +637,15 @@ __device__ __forceinline__ int sky_fused_mask(int kind) {
 
 // Shading and fog of the shaded family (kernels.cu:271-292, 446-469).
 template <int KIND>
-__device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*rgb)[3], const float* sky, float out[3]) {
+__device__ __forceinline__ void shade_rgb(const Hit& h, float vd, float rcp_vd, const float (*rgb)[3], const float* sky,
+                                          float out[3]) {
     if (h.blk >= 0) {
         float r = rgb[h.blk][0], g = rgb[h.blk][1], b_col = rgb[h.blk][2];
         float shade = 1.0f;
         if (h.face == 0) shade = 0.8f;
         else if (h.face == 2) shade = 0.9f;
         else if (h.face == 1 && h.step_y < 0) shade = 0.6f;
-        float fog = fminf(N::div(h.t, vd), 1.0f);
+        float fog = fminf(N::div_r(h.t, vd, rcp_vd), 1.0f);
         fog = N::mul(fog, fog);
         float omf = N::sub(1.0f, fog);
         const int m = sky_fused_mask(KIND);
@@ -617,14 +662,19 @@ __device__ __forceinline__ void shade_rgb(const Hit& h, float vd, const float (*
     }
 }
 
-__device__ __forceinline__ uint32_t to_u8(float x) { return (uint32_t)(uint8_t)N::mul(x, 255.0f); }
+// (uint8_t)(x * 255) for x*255 in [0, 256): adding 2^23 with round-toward-
+// zero leaves trunc(x*255) in the low mantissa bits, which is the C++
+// float-to-integer conversion without using the conversion unit.
+__device__ __forceinline__ uint32_t to_u8(float x) {
+    return __float_as_uint(__fadd_rz(N::mul(x, 255.0f), 8388608.0f)) & 0xffu;
+}
 
 // Flat ray of render_kernel_uint8_minimal / _prebasis / _smem
 // (kernels.cu:1036-1097, 619-679): rsqrtf normalisation, no AABB, no fog,
 // unsigned bounds test, non-cubic world.
 template <bool TRIG, class V>
-__device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
-                                        int max_steps) {
+__device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
+                                        int wz, int max_steps, bool skip_first = false) {
     float ray_x, ray_y, ray_z;
     ray_dir<TRIG>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
@@ -632,9 +682,7 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
     ray_y = N::mul(ray_y, ray_len);
     ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
-    int vx = (int)floorf(c.eye_x);
-    int vy = (int)floorf(c.eye_y);
-    int vz = (int)floorf(c.eye_z);
+    int vx = d0.vx, vy = d0.vy, vz = d0.vz;
     int sx = (ray_x >= 0) ? 1 : -1;
     int sy = (ray_y >= 0) ? 1 : -1;
     int sz = (ray_z >= 0) ? 1 : -1;
@@ -642,29 +690,33 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
     float iy = (ray_y != 0.0f) ? N::div(1.0f, ray_y) : 1e30f;
     float iz = (ray_z != 0.0f) ? N::div(1.0f, ray_z) : 1e30f;
     float tdx = fabsf(ix), tdy = fabsf(iy), tdz = fabsf(iz);
-    float tmx = N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ix);
-    float tmy = N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iy);
-    float tmz = N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), iz);
+    float tmx = N::mul((ray_x >= 0) ? d0.nxp : d0.nxm, ix);
+    float tmy = N::mul((ray_y >= 0) ? d0.nyp : d0.nym, iy);
+    float tmz = N::mul((ray_z >= 0) ? d0.nzp : d0.nzm, iz);
     Hit h;
     h.blk = AIR;
     h.face = -1;
     h.t = 0.0f;
     h.step_y = sy;
     int face = -1;
+    int idx = vy * wxz + vx * wz + vz;
+    const int dix = sx * wz, diy = sy * wxz, diz = sz;
     for (int step = 0; step < max_steps; ++step) {
-        if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
-            int8_t b = vox(vy * wxz + vx * wz + vz);
+        // skip_first: the eye's voxel is known to be air or outside the world
+        if ((step > 0 || !skip_first) &&
+            (unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
+            int8_t b = vox(idx);
             if (b >= 0) {
                 h.blk = b;
                 break;
             }
         }
         if (tmx < tmy && tmx < tmz) {
-            tmx = N::add(tmx, tdx); vx += sx; face = 0;
+            tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0;
         } else if (tmy < tmz) {
-            tmy = N::add(tmy, tdy); vy += sy; face = 1;
+            tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1;
         } else {
-            tmz = N::add(tmz, tdz); vz += sz; face = 2;
+            tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2;
         }
     }
     h.face = face;
@@ -674,8 +726,8 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, float u, float v, const V&
 // render_kernel_uint8_fp16 (kernels.cu:1176-1248): the DDA's t_max/t_delta
 // in binary16 (inverse 65504 for a zero component).
 template <class V>
-__device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V& vox, int wx, int wy, int wz,
-                                        int max_steps) {
+__device__ __forceinline__ Hit fp16_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
+                                        int wz, int max_steps) {
     float ray_x, ray_y, ray_z;
     ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
@@ -683,9 +735,7 @@ __device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V&
     ray_y = N::mul(ray_y, ray_len);
     ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
-    int vx = (int)floorf(c.eye_x);
-    int vy = (int)floorf(c.eye_y);
-    int vz = (int)floorf(c.eye_z);
+    int vx = d0.vx, vy = d0.vy, vz = d0.vz;
     int sx = (ray_x >= 0) ? 1 : -1;
     int sy = (ray_y >= 0) ? 1 : -1;
     int sz = (ray_z >= 0) ? 1 : -1;
@@ -695,9 +745,9 @@ __device__ __forceinline__ Hit fp16_ray(const Cam& c, float u, float v, const V&
     __half tdx = __float2half(fabsf(ixf));
     __half tdy = __float2half(fabsf(iyf));
     __half tdz = __float2half(fabsf(izf));
-    __half tmx = __float2half(N::mul((ray_x >= 0) ? N::sub((float)(vx + 1), c.eye_x) : N::sub((float)vx, c.eye_x), ixf));
-    __half tmy = __float2half(N::mul((ray_y >= 0) ? N::sub((float)(vy + 1), c.eye_y) : N::sub((float)vy, c.eye_y), iyf));
-    __half tmz = __float2half(N::mul((ray_z >= 0) ? N::sub((float)(vz + 1), c.eye_z) : N::sub((float)vz, c.eye_z), izf));
+    __half tmx = __float2half(N::mul((ray_x >= 0) ? d0.nxp : d0.nxm, ixf));
+    __half tmy = __float2half(N::mul((ray_y >= 0) ? d0.nyp : d0.nym, iyf));
+    __half tmz = __float2half(N::mul((ray_z >= 0) ? d0.nzp : d0.nzm, izf));
     Hit h;
     h.blk = AIR;
     h.face = -1;
@@ -855,9 +905,9 @@ __global__ void __launch_bounds__(128) k_render_shaded(mc_kp p) {
     float u = u_shaded(px, p.W, p.H, p.fov);
     float v = v_shaded(py, p.H, p.fov);
     VoxLdg vox{p.voxels + b * (long long)p.wx * p.wy * p.wz};
-    Hit h = shade_ray<FASTG>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
+    Hit h = shade_ray<FASTG>(c, dda0(c), u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
     float rgb[3];
-    shade_rgb<F32 ? MC_COL_F32 : (FASTG ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, c_rgb, c_sky, rgb);
+    shade_rgb<F32 ? MC_COL_F32 : (FASTG ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, N::rcp_of(p.vd), c_rgb, c_sky, rgb);
     if (F32) {
         float* o = (float*)p.obs + idx * 3;
         o[0] = rgb[0]; o[1] = rgb[1]; o[2] = rgb[2];
@@ -899,9 +949,10 @@ __global__ void __launch_bounds__(128) k_render_flat(mc_kp p) {
     long long wxyz = (long long)p.wx * p.wy * p.wz;
     VoxLdg vox{p.voxels + b * wxyz};
     Hit h;
-    if (FAM == MC_FAM_FP16) h = fp16_ray(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
-    else if (FAM == MC_FAM_PREBASIS) h = flat_ray<false>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
-    else h = flat_ray<true>(c, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    const Dda0 d0 = dda0(c);
+    if (FAM == MC_FAM_FP16) h = fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    else if (FAM == MC_FAM_PREBASIS) h = flat_ray<false>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    else h = flat_ray<true>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     long long o = (b * hw + pix);
     uint8_t* out = (uint8_t*)p.obs + o * 3;
     const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
@@ -931,7 +982,7 @@ __global__ void __launch_bounds__(128) k_render_coalesced(const int8_t* vox, con
             return __ldg(v + (long long)idx * B + b);
         }
     } acc{vox, B, b, ws};
-    Hit h = flat_ray<false>(c, u, v, acc, ws, ws, ws, max_steps);
+    Hit h = flat_ray<false>(c, dda0(c), u, v, acc, ws, ws, ws, max_steps);
     const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
     uint8_t* o = out + ((long long)b * H * W + pix) * 3;
     o[0] = col[0]; o[1] = col[1]; o[2] = col[2];
@@ -941,11 +992,14 @@ __global__ void __launch_bounds__(128) k_render_coalesced(const int8_t* vox, con
 // Fused form: one persistent kernel per step, one warp per env
 // ---------------------------------------------------------------------------
 // Shared memory layout (per CTA): u/v tables, colour tables, then per warp a
-// pixel staging buffer, an mbarrier and (stage=1) one world.
+// pixel staging buffer, an mbarrier and (stage=1) one world.  A warp marches
+// one tile of tile_w x (32/tile_w) pixels per iteration (nearby rays have
+// similar lengths, which keeps the lanes of the DDA loop together) and
+// stages a band of 32/tile_w full image rows, written out contiguously.
 struct FusedLayout {
     int W, H;
-    int chunk_px;      // pixels per chunk (32 * px_per_lane)
-    int stage_bytes;   // staging bytes per warp
+    int tile_w, tile_h;
+    int stage_bytes;   // staging bytes per warp (one band of rows)
     int world_bytes;   // world bytes per warp (0 when not staged)
     int warp_bytes;    // total per warp (16-aligned)
     int head_bytes;    // tables (16-aligned)
@@ -953,12 +1007,13 @@ struct FusedLayout {
 
 __host__ __device__ inline int mc_align16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int obs_f32, int stage, int ppl) {
+__host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int obs_f32, int stage, int tile_w) {
     FusedLayout L;
     L.W = W;
     L.H = H;
-    L.chunk_px = 32 * ppl;
-    L.stage_bytes = mc_align16(L.chunk_px * 3 * (obs_f32 ? 4 : 1));
+    L.tile_w = tile_w;
+    L.tile_h = 32 / tile_w;
+    L.stage_bytes = mc_align16(W * L.tile_h * 3 * (obs_f32 ? 4 : 1));
     L.world_bytes = stage ? mc_align16(wxyz) : 0;
     L.warp_bytes = 16 + L.stage_bytes + L.world_bytes;  // 16: mbarrier
     L.head_bytes = mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
@@ -1006,8 +1061,11 @@ __device__ __forceinline__ long long next_env(const mc_kp& p, long long cur, lon
     return (long long)__shfl_sync(0xffffffffu, v, 0);
 }
 
-template <int FAM, bool F32, bool STAGE, int PPL>
-__global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
+#ifndef MC_FUSED_MIN_BLOCKS
+#define MC_FUSED_MIN_BLOCKS 4
+#endif
+template <int FAM, bool F32, bool STAGE>
+__global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p, int tile_w) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -1016,7 +1074,7 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
     const int HW = W * H;
     const int wxz = p.wx * p.wz;
     const int wxyz = wxz * p.wy;
-    FusedLayout L = fused_layout(W, H, wxyz, F32, STAGE, PPL);
+    FusedLayout L = fused_layout(W, H, wxyz, F32, STAGE, tile_w);
 
     // --- tables -------------------------------------------------------------
     float* s_u = reinterpret_cast<float*>(smem);
@@ -1058,6 +1116,7 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
     uint32_t phase = 0;
     bool any_done = false;
     bool failed = false;
+    const float rcp_vd = N::rcp_of(p.vd);
 
     const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
     const long long total_warps = (long long)gridDim.x * nwarps;
@@ -1129,6 +1188,14 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
         } else {
             buried = p.max_steps > 0 && eye_inb && eye_blk >= 0;
         }
+        // not buried: the first DDA step of every ray tests the eye voxel and
+        // advances; when that test is known to fail, rays start advanced
+        bool skip_first;
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST)
+            skip_first = inside && p.vd > 0.0f && p.max_steps > 0 && eye_blk < 0 &&
+                         !(FAM == MC_FAM_SHADED_FAST && ey < p.gh);
+        else
+            skip_first = p.max_steps > 0 && !(eye_inb && eye_blk >= 0);
         uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
         const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
         if (buried) {
@@ -1140,8 +1207,8 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
             uint8_t bytes[12];
             if (F32 || FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                 float rgb[3];
-                shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, s_rgb,
-                                                                                                      s_sky, rgb);
+                shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, rcp_vd,
+                                                                                                      s_rgb, s_sky, rgb);
                 if (F32) {
                     // pattern period 12 bytes
 #pragma unroll
@@ -1207,34 +1274,34 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
             wsrc = sworld;
         }
         // ---- march every pixel ---------------------------------------------
-        const int nchunks = (HW + L.chunk_px - 1) / L.chunk_px;
-        for (int ch = 0; ch < nchunks; ++ch) {
-            const int base = ch * L.chunk_px;
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) {
-                const int pix = base + j * 32 + lane;
-                if (pix < HW) {
-                    const int py = pix / W;
-                    const int px = pix - py * W;
+        const Dda0 d0 = dda0(c);
+        const int TW = L.tile_w, TH = L.tile_h;
+        const int lx = lane % TW, ly = lane / TW;
+        const int bpp = 3 * (F32 ? 4 : 1);  // bytes per pixel
+        for (int row0 = 0; row0 < H; row0 += TH) {
+            const int py = row0 + ly;
+            const float v = (py < H) ? s_v[py] : 0.0f;
+            for (int tx0 = 0; tx0 < W; tx0 += TW) {
+                const int px = tx0 + lx;
+                if (px < W && py < H) {
                     Hit h;
                     const float u = s_u[px];
-                    const float v = s_v[py];
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
-                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
-                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside);
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first);
+                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first);
                     } else if (FAM == MC_FAM_FP16) {
-                        if (STAGE) h = fp16_ray(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
-                        else h = fp16_ray(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        if (STAGE) h = fp16_ray(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     } else {
                         constexpr bool TRIG = (FAM != MC_FAM_PREBASIS);
-                        if (STAGE) h = flat_ray<TRIG>(c, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
-                        else h = flat_ray<TRIG>(c, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
+                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first);
+                        else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first);
                     }
-                    const int so = (j * 32 + lane);
+                    const int so = ly * W + px;  // pixel within the staged band
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         float rgb[3];
                         shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
-                            h, p.vd, s_rgb, s_sky, rgb);
+                            h, p.vd, rcp_vd, s_rgb, s_sky, rgb);
                         if (F32) {
                             float* sf = reinterpret_cast<float*>(stage) + so * 3;
                             sf[0] = rgb[0]; sf[1] = rgb[1]; sf[2] = rgb[2];
@@ -1249,15 +1316,14 @@ __global__ void __launch_bounds__(256, 4) k_step_fused(mc_kp p) {
                         uint8_t* sb = stage + so * 3;
                         sb[0] = col[0]; sb[1] = col[1]; sb[2] = col[2];
                     }
-                    if (p.dbg_pixel) p.dbg_pixel[e * HW + pix] = dbg_code(h);
+                    if (p.dbg_pixel) p.dbg_pixel[e * HW + py * W + px] = dbg_code(h);
                 }
             }
             __syncwarp();
-            // copy the chunk out
-            const int npx = min(L.chunk_px, HW - base);
-            const int nbytes = npx * 3 * (F32 ? 4 : 1);
-            uint8_t* dst = oenv + (long long)base * 3 * (F32 ? 4 : 1);
-            if (vec_ok && (nbytes & 15) == 0) {
+            // copy the band (rows row0 .. row0+TH-1) out
+            const int nbytes = min(TH, H - row0) * W * bpp;
+            uint8_t* dst = oenv + (long long)row0 * W * bpp;
+            if (vec_ok && (nbytes & 15) == 0 && (((long long)row0 * W * bpp) & 15) == 0) {
                 const uint4* s4 = reinterpret_cast<const uint4*>(stage);
                 uint4* d4 = reinterpret_cast<uint4*>(dst);
                 for (int k = lane; k < (nbytes >> 4); k += 32) d4[k] = s4[k];
@@ -1336,13 +1402,13 @@ static int step_plain(const mc_kp* p, cudaStream_t s) {
 
 static size_t fused_smem(const mc_kp* p, const mc_fused_cfg* cfg) {
     int wxyz = p->wx * p->wy * p->wz;
-    FusedLayout L = fused_layout(p->W, p->H, wxyz, p->obs_f32, cfg->stage, cfg->px_per_lane);
+    FusedLayout L = fused_layout(p->W, p->H, wxyz, p->obs_f32, cfg->stage, cfg->tile_w);
     return (size_t)L.head_bytes + (size_t)cfg->warps_per_cta * L.warp_bytes;
 }
 
-template <int FAM, bool F32, bool STAGE, int PPL>
+template <int FAM, bool F32, bool STAGE>
 static int launch_fused_t(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
-    auto kern = k_step_fused<FAM, F32, STAGE, PPL>;
+    auto kern = k_step_fused<FAM, F32, STAGE>;
     size_t smem = fused_smem(p, cfg);
     static size_t attr_set = 0;  // per instantiation
     if (smem > 48 * 1024 && smem > attr_set) {
@@ -1355,18 +1421,14 @@ static int launch_fused_t(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, 
     long long grid = (long long)num_sms * (cfg->ctas_per_sm > 0 ? cfg->ctas_per_sm : 1);
     if (grid > ctas_needed) grid = ctas_needed;
     if (grid < 1) grid = 1;
-    kern<<<(unsigned)grid, threads, smem, s>>>(*p);
+    kern<<<(unsigned)grid, threads, smem, s>>>(*p, cfg->tile_w);
     return (int)cudaGetLastError();
 }
 
 template <int FAM, bool F32>
 static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
-    const bool st = cfg->stage != 0;
-    switch (cfg->px_per_lane) {
-        case 1: return st ? launch_fused_t<FAM, F32, true, 1>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 1>(p, cfg, num_sms, s);
-        case 2: return st ? launch_fused_t<FAM, F32, true, 2>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 2>(p, cfg, num_sms, s);
-        default: return st ? launch_fused_t<FAM, F32, true, 4>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, false, 4>(p, cfg, num_sms, s);
-    }
+    return cfg->stage ? launch_fused_t<FAM, F32, true>(p, cfg, num_sms, s)
+                      : launch_fused_t<FAM, F32, false>(p, cfg, num_sms, s);
 }
 
 static int step_fused(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {

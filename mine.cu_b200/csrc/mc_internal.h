@@ -83,7 +83,7 @@ struct mc_fused_cfg {
     int stage;          // 1: copy each rendered world into shared memory with a bulk copy; 0: read voxels from L1/L2
     int warps_per_cta;  // 4 or 8
     int ctas_per_sm;    // persistent grid = SMs * ctas_per_sm
-    int px_per_lane;    // pixels per lane per chunk (1, 2, 4)
+    int tile_w;         // march tiles of tile_w x (32/tile_w) pixels (8, 16 or 32)
 };
 
 // One numerics back end (ref_fast or ieee).

@@ -413,14 +413,14 @@ static void default_fused(mc_env* e) {
     e->fcfg.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
     e->fcfg.warps_per_cta = 8;
     e->fcfg.ctas_per_sm = 4;
-    e->fcfg.px_per_lane = 4;
+    e->fcfg.tile_w = 8;
 }
 
 static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
     if (f->warps_per_cta != 4 && f->warps_per_cta != 8)
         return fail(MC_ERR_INVALID, "warps_per_cta must be 4 or 8");
-    if (f->px_per_lane != 1 && f->px_per_lane != 2 && f->px_per_lane != 4)
-        return fail(MC_ERR_INVALID, "px_per_lane must be 1, 2 or 4");
+    if (f->tile_w != 4 && f->tile_w != 8 && f->tile_w != 16 && f->tile_w != 32)
+        return fail(MC_ERR_INVALID, "tile_w must be 4, 8, 16 or 32");
     if (f->ctas_per_sm < 1 || f->ctas_per_sm > 32) return fail(MC_ERR_INVALID, "ctas_per_sm out of range");
     int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
     if (f->stage && (wxyz & 15)) return fail(MC_ERR_INVALID, "stage needs world bytes %% 16 == 0");
@@ -601,7 +601,7 @@ extern "C" int mc_env_render(mc_env* e, void* stream) {
 
 static bool same_fcfg(const mc_fused_cfg& a, const mc_fused_cfg& b) {
     return a.stage == b.stage && a.warps_per_cta == b.warps_per_cta && a.ctas_per_sm == b.ctas_per_sm &&
-           a.px_per_lane == b.px_per_lane;
+           a.tile_w == b.tile_w;
 }
 
 static int rollout_graph(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
@@ -685,7 +685,7 @@ extern "C" int mc_env_rollout(mc_env* e, const uint8_t* actions, int32_t K, floa
 
 extern "C" int mc_env_set_fused_config(mc_env* e, const mc_fused_config* c) {
     if (!e || !c) return fail(MC_ERR_INVALID, "NULL argument");
-    mc_fused_cfg f{c->stage, c->warps_per_cta, c->ctas_per_sm, c->px_per_lane};
+    mc_fused_cfg f{c->stage, c->warps_per_cta, c->ctas_per_sm, c->tile_w};
     int rc = validate_fused(e, &f);
     if (rc) return rc;
     e->fcfg = f;
@@ -697,7 +697,7 @@ extern "C" int mc_env_get_fused_config(const mc_env* e, mc_fused_config* c) {
     c->stage = e->fcfg.stage;
     c->warps_per_cta = e->fcfg.warps_per_cta;
     c->ctas_per_sm = e->fcfg.ctas_per_sm;
-    c->px_per_lane = e->fcfg.px_per_lane;
+    c->tile_w = e->fcfg.tile_w;
     return MC_OK;
 }
 
@@ -890,7 +890,7 @@ extern "C" int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* s
         f.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
         f.warps_per_cta = 8;
         f.ctas_per_sm = 4;
-        f.px_per_lane = 4;
+        f.tile_w = 8;
         return backend_rc(be->step_fused(&k, &f, sms, (cudaStream_t)stream), "step_fused");
     }
     return fail(MC_ERR_INVALID, "unknown form %d", form);

@@ -490,8 +490,8 @@ void env_rollout_prepare(std::shared_ptr<Env> e, torch::Tensor actions, c10::opt
        "rollout_prepare");
 }
 
-void env_set_fused(std::shared_ptr<Env> e, int stage, int warps_per_cta, int ctas_per_sm, int px_per_lane) {
-    mc_fused_config f{stage, warps_per_cta, ctas_per_sm, px_per_lane};
+void env_set_fused(std::shared_ptr<Env> e, int stage, int warps_per_cta, int ctas_per_sm, int tile_w) {
+    mc_fused_config f{stage, warps_per_cta, ctas_per_sm, tile_w};
     ck(mc_env_set_fused_config(e->h, &f), "set_fused_config");
 }
 
@@ -502,7 +502,7 @@ py::dict env_get_fused(std::shared_ptr<Env> e) {
     d["stage"] = f.stage;
     d["warps_per_cta"] = f.warps_per_cta;
     d["ctas_per_sm"] = f.ctas_per_sm;
-    d["px_per_lane"] = f.px_per_lane;
+    d["tile_w"] = f.tile_w;
     d["smem_bytes"] = mc_env_fused_smem_bytes(e->h);
     return d;
 }

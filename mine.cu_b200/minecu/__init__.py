@@ -344,9 +344,9 @@ class MineEnv:
         return (self.render_height, self.render_width, 3)
 
     # ------------------------------------------------------------------
-    def set_launch_config(self, stage: int, warps_per_cta: int, ctas_per_sm: int, px_per_lane: int) -> None:
+    def set_launch_config(self, stage: int, warps_per_cta: int, ctas_per_sm: int, tile_w: int) -> None:
         """Launch shape of the fused kernel (see minecu.autotune)."""
-        _C.env_set_fused(self._env, int(stage), int(warps_per_cta), int(ctas_per_sm), int(px_per_lane))
+        _C.env_set_fused(self._env, int(stage), int(warps_per_cta), int(ctas_per_sm), int(tile_w))
 
     def launch_config(self) -> dict:
         return _C.env_get_fused(self._env)

@@ -47,7 +47,7 @@ class EnvState(ctypes.Structure):
 
 class FusedConfig(ctypes.Structure):
     _fields_ = [("stage", c_int32), ("warps_per_cta", c_int32), ("ctas_per_sm", c_int32),
-                ("px_per_lane", c_int32)]
+                ("tile_w", c_int32)]
 
 
 class DecodeBuffers(ctypes.Structure):
