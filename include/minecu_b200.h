@@ -219,6 +219,20 @@ int mc_raycast_break(int8_t* voxels, const float* positions, const float* yaws, 
                      const uint8_t* do_break, float* rewards, int32_t B, int32_t world_size, int32_t target_block,
                      float reward_value, int32_t numerics, void* stream);
 
+/* ---- allocation-free step (no counterpart in the reference) -----------
+ * For callers that cannot allocate device memory (fixed memory budgets,
+ * allocators owned by another runtime): the plain step of
+ * mc_step_stateless(..., MC_FORM_PLAIN), with its action-decode scratch and
+ * flag words in a static device array inside the library instead of caller
+ * buffers or lazy allocations.  At most MC_NOALLOC_MAX_ENVS envs per call
+ * (larger batches are rejected with MC_ERR_INVALID); the array (about
+ * 1.5 MB) stays on every GPU that loads the library until exit.  The first
+ * call on a device looks up the array's address: make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race. */
+#define MC_NOALLOC_MAX_ENVS 65536
+int mc_step_plain_noalloc(const mc_env_config* cfg, const mc_env_state* state, const int8_t* buttons,
+                          const float* look, void* stream);
+
 /* ---- synthetic action stream (no reference counterpart: the benchmark's
  *      seeded Philox4x32-10 actions, docs/environment.md:5-17 table) ----- */
 int mc_philox_actions(uint8_t* actions, int32_t B, int32_t K, int32_t env_offset, int32_t step0, uint64_t seed,

@@ -34,6 +34,7 @@ UNITS = {
     "mc_fast": ["--use_fast_math"],
     "mc_ieee": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "mc_runtime": [],
+    "mc_noalloc": [],
 }
 
 

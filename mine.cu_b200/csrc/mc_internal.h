@@ -109,3 +109,14 @@ extern "C" const mc_backend* mc_backend_ieee();
 // numerics-independent kernels (mc_runtime.cu)
 int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s);
 int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s);
+
+// Record an error message for mc_last_error() and return `code`.
+int mc_set_error(int code, const char* msg);
+// mc_step_stateless with the flag words supplied by the caller (no lazy
+// allocation of the per-device flag block).
+struct mc_env_config;
+struct mc_env_state;
+struct mc_decode_buffers;
+int mc_step_stateless_with_flags(const mc_env_config* cfg, const mc_env_state* st, const int8_t* buttons,
+                                 const float* look, const mc_decode_buffers* dec, int32_t* flags, int form,
+                                 void* stream);

@@ -49,6 +49,8 @@ static int backend_rc(int rc, const char* what) {
     return cuda_fail((cudaError_t)rc, what);
 }
 
+int mc_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" int mc_abi_version(void) { return MC_ABI_VERSION; }
 extern "C" const char* mc_last_error(void) { return g_err; }
 
@@ -978,4 +980,31 @@ extern "C" int mc_discrete_to_buttons(const uint8_t* actions, int32_t B, float l
     k_discrete<<<blocks(B, 256), 256, 0, (cudaStream_t)stream>>>(actions, B, look_delta, buttons, look);
     MC_CK(cudaGetLastError());
     return MC_OK;
+}
+
+int mc_step_stateless_with_flags(const mc_env_config* cfg, const mc_env_state* st, const int8_t* buttons,
+                                 const float* look, const mc_decode_buffers* dec, int32_t* flags, int form,
+                                 void* stream) {
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    rc = check_state(cfg, st);
+    if (rc) return rc;
+    if (cfg->batch_size == 0) return MC_OK;
+    if (!buttons || !look) return fail(MC_ERR_INVALID, "buttons/look are NULL");
+    if (form != MC_FORM_PLAIN || !dec || !flags) return fail(MC_ERR_INVALID, "plain form with decode buffers and flags");
+    mc_kp k;
+    fill_kp(&k, cfg, st);
+    k.ext_done = (cfg->obs_mode == MC_OBS_UINT8_PREBASIS_FULL) ? 0 : 1;
+    k.buttons = buttons;
+    k.look = look;
+    k.flags = flags;
+    k.s_fwd = dec->forward_in;
+    k.s_strafe = dec->strafe_in;
+    k.s_dyaw = dec->delta_yaw_in;
+    k.s_dpitch = dec->delta_pitch_in;
+    k.s_jump = dec->jump_in;
+    k.s_brk = dec->do_break;
+    k.s_place = dec->do_place;
+    k.s_speed = dec->speed_mult;
+    return backend_rc(backend_of(cfg->numerics)->step_plain(&k, (cudaStream_t)stream), "step_plain");
 }

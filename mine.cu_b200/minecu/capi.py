@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(_HERE, "libminecu_b200.so")
 HEADER = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "minecu_b200.h")
 
 MC_OK, MC_ERR_INVALID, MC_ERR_CUDA, MC_ERR_KERNEL, MC_ERR_UNSUPPORTED = 0, -1, -2, -3, -4
+NOALLOC_MAX_ENVS = 65536
 NUMERICS_REF_FAST, NUMERICS_IEEE = 0, 1
 FORM_PLAIN, FORM_FUSED = 0, 1
 OBS = dict(float32=0, uint8=1, uint8_minimal=2, uint8_fp16=3, uint8_prebasis=4, uint8_prebasis_full=5,
@@ -87,6 +88,7 @@ _PROTOS = {
     "mc_step_stateless": (I, [PCFG, PST, P, P, ctypes.POINTER(DecodeBuffers), I, P]),
     "mc_physics": (I, [P, P, P, P, P, P, P, P, P, P, P, I, I, F, F, F, F, I, P]),
     "mc_raycast_break": (I, [P, P, P, P, P, P, I, I, I, F, I, P]),
+    "mc_step_plain_noalloc": (I, [PCFG, PST, P, P, P]),
     "mc_philox_actions": (I, [P, I, I, I, I, U64, I, P]),
     "mc_discrete_to_buttons": (I, [P, I, F, P, P, P]),
 }
