@@ -287,6 +287,187 @@ def run_mine(args):
         dist.destroy_process_group()
 
 
+# Ragged batch: 24,576 envs in 6 uneven groups (batch, world edge, square
+# resolution), uint8 shaded observations, discrete actions seed 3.  The
+# 8^3 group uses ground height 4 (half its height); with the default 8 its
+# whole world would be solid ground.
+RAGGED_GROUPS = [(8192, 8, 16), (6144, 16, 32), (4096, 16, 64), (3072, 24, 32), (2048, 32, 32), (1024, 32, 64)]
+RAGGED_SEED = 3
+RAGGED_METRIC = "env-steps/s, ragged batch of 24,576 envs in 6 groups (one persistent launch, CUDA graph)"
+
+
+def ragged_ground(w: int) -> int:
+    return min(8, w // 2)
+
+
+def ragged_bytes_per_step(groups=RAGGED_GROUPS) -> int:
+    return sum(b * (w ** 3 + r * r * 3) for b, w, r in groups)
+
+
+def ragged_cpu_baseline(seconds=12.0, scale=16):
+    """The oracle (IEEE numerics, OpenMP over envs) on a bounded sample of
+    the ragged workload: every group at 1/`scale` of its batch, stepped
+    until `seconds` have passed; env-steps/s summed over the groups."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    envs = []
+    for b, w, r in RAGGED_GROUPS:
+        e = O.OracleEnv(batch_size=b // scale, world_size=w, render_width=r, render_height=r,
+                        ground_height=ragged_ground(w), obs_dtype="uint8", threads=cores)
+        e.reset()
+        envs.append(e)
+    total = sum(e.B for e in envs)
+    acts = [O.discrete_to_buttons(O.philox_actions(total, s, RAGGED_SEED), 0.1) for s in range(16)]
+    n, t0 = 0, time.perf_counter()
+    while True:
+        btn, look = acts[n % 16]
+        o = 0
+        for e in envs:
+            e.step(btn[o:o + e.B], look[o:o + e.B])
+            o += e.B
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    return {"value": total * n / el, "unit": "env-steps/s", "cores": cores, "kind": "port",
+            "sample": f"the 6 groups at 1/{scale} of their batch ({total} envs) x {n} steps ({el:.1f} s), "
+                      f"oracle/mc_oracle.c with {cores} OpenMP threads"}
+
+
+def run_mine_ragged(args):
+    import torch
+    from minecu import MineEnv, _C
+    from minecu.ragged import RaggedBatch
+    from minecu import autotune
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    K, Wm = args.steps, args.warmup
+
+    def make(form):
+        return [MineEnv(batch_size=b, world_size=w, render_width=r, render_height=r, device=str(dev),
+                        ground_height=ragged_ground(w), obs_dtype="uint8", numerics="ref_fast", form=form)
+                for b, w, r in RAGGED_GROUPS]
+
+    envs = make("fused")
+    batch = RaggedBatch(envs)
+    total = batch.total
+    t_tune = time.perf_counter()
+    tuned = autotune.tune_ragged(batch, use_cache=False)
+    t_tune = time.perf_counter() - t_tune
+    acts_w = torch.empty((Wm, total), dtype=torch.uint8, device=dev)
+    acts_t = torch.empty((K, total), dtype=torch.uint8, device=dev)
+    _C.philox_actions(acts_w, rank * total, 0, RAGGED_SEED)
+    _C.philox_actions(acts_t, rank * total, Wm, RAGGED_SEED)
+    batch.prepare_rollout(acts_w)
+    batch.prepare_rollout(acts_t)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+
+    # ---- ragged: one persistent launch per step, K steps in one graph -------
+    batch.reset()
+    batch.rollout(acts_w)
+    with ClockSampler(local) as clk:
+        t_ragged = timed(lambda: batch.rollout(acts_t))
+    batch.check_error()
+    value = total * K * world / t_ragged
+
+    # ---- the groups as separate fused launches (6 graphs per K steps) -------
+    sl = [batch.group_slice(g) for g in range(len(envs))]
+    gw = [acts_w[:, x].contiguous() for x in sl]
+    gt = [acts_t[:, x].contiguous() for x in sl]
+    for g, e in enumerate(envs):
+        c = tuned["config"]
+        team = c["team_warps"] if c["coop"][g] else 1
+        e.set_launch_config(c["stage"][g], 8, 4, c["tile_w"][g], team_warps=team, coop=c["coop"][g])
+        e.prepare_rollout(gw[g])
+        e.prepare_rollout(gt[g])
+        e.reset()
+        e.rollout(gw[g])
+    t_sep_fused = timed(lambda: [e.rollout(gt[g]) for g, e in enumerate(envs)])
+
+    # ---- the groups as separate plain launches (the reference's sequence) ---
+    for e in envs:
+        e.form = "plain"
+        e.reset()
+    for s in range(Wm):
+        for g, e in enumerate(envs):
+            e.step(gw[g][s])
+    t_plain = timed(lambda: [e.step(gt[g][s]) for s in range(K) for g, e in enumerate(envs)])
+    for e in envs:
+        e.form = "fused"
+
+    # ---- e2e: RaggedBatch.step with host buffers ----------------------------
+    h_acts = torch.cat([acts_w, acts_t]).cpu().pin_memory()
+    h_rew = torch.empty((K, total), dtype=torch.float32).pin_memory()
+    h_done = torch.empty((K, total), dtype=torch.bool).pin_memory()
+    d_act = torch.empty((total,), dtype=torch.uint8, device=dev)
+    batch.reset()
+    for s in range(Wm):
+        d_act.copy_(h_acts[s], non_blocking=True)
+        batch.step(d_act)
+
+    def e2e_loop():
+        for s in range(K):
+            d_act.copy_(h_acts[Wm + s], non_blocking=True)
+            res = batch.step(d_act)
+            for g, (obs, rew, done) in enumerate(res):
+                h_rew[s, sl[g]].copy_(rew, non_blocking=True)
+                h_done[s, sl[g]].copy_(done, non_blocking=True)
+
+    t_e2e = timed(e2e_loop)
+    _ = float(h_rew.sum())
+
+    peak, peak_kind = load_peaks()
+    bps = ragged_bytes_per_step()
+    achieved = bps / (t_ragged / K) / 1e9
+    line = {
+        "metric": RAGGED_METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": t_ragged / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (reference world generator, Philox actions seed 3)",
+        "config": {"workload": "ragged: groups (batch, world, res) " + ", ".join(
+            f"({b}, {w}^3, {r}x{r})" for b, w, r in RAGGED_GROUPS) + "; uint8 shaded obs; 8^3 ground height 4",
+                   "global_batch": total * world, "numerics": "ref_fast", "launch": tuned["config"],
+                   "autotune": {"trials": tuned["trials"], "seconds": round(t_tune, 1)},
+                   "parallelism": f"env-sharded x{world} (no collective)",
+                   "trajectory": f"steps {Wm}..{Wm + K - 1} after reset(), every arm",
+                   "l2": f"per-step working set {bps / 1e6:.0f} MB > 126 MB L2; no flush"},
+        "separate_fused": {"value": total * K * world / t_sep_fused, "unit": "env-steps/s",
+                           "ms_per_step": t_sep_fused / K * 1e3,
+                           "form": "6 fused launches per step (one graph per group, each with the group's "
+                                   "tuned tile/staging/team choice)"},
+        "separate_plain": {"value": total * K * world / t_plain, "unit": "env-steps/s",
+                           "ms_per_step": t_plain / K * 1e3, "ragged_speedup": t_plain / t_ragged,
+                           "form": "6 groups x the reference's kernel sequence per step (eager)"},
+        "e2e": {"value": total * K * world / t_e2e, "unit": "env-steps/s", "h2d_bytes_per_step": total,
+                "d2h_bytes_per_step": total * 5,
+                "path": "RaggedBatch.step(actions); pinned H2D actions, D2H rewards+dones"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_step": bps,
+                     "kernel": "k_step_ragged (avg over the timed region)"},
+        "gpu_launches": K * (1 + sum(1 for e in envs if e.episode_length)),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = ragged_cpu_baseline(args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def run_reference(args):
     """The reference's own CUDA build (oracle/_ref/libminecu_ref.so, its
     src/kernels.cu compiled unmodified) driven in its MineEnv.step order, on
@@ -360,6 +541,90 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_ragged(args):
+    """The ragged workload on the reference's own CUDA build: the reference
+    runs one world size and resolution per MineEnv, so the 6 groups are 6
+    envs stepped one after another each step (its plain per-group form)."""
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import ref_driver
+    if not ref_driver.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libminecu_ref.so not built"}))
+        return
+    K, Wm = args.steps, args.warmup
+    dev = torch.device("cuda", local)
+    envs = [ref_driver.RefEnv(batch_size=b, world_size=w, render_width=r, render_height=r, device=str(dev),
+                              ground_height=ragged_ground(w), obs_dtype="uint8", target_block=3)
+            for b, w, r in RAGGED_GROUPS]
+    total = sum(b for b, _, _ in RAGGED_GROUPS)
+    btns = torch.empty((K + Wm, total, 8), dtype=torch.int8)
+    looks = torch.empty((K + Wm, total, 2), dtype=torch.float32)
+    for s in range(K + Wm):
+        b, l = O.discrete_to_buttons(O.philox_actions(total, s, RAGGED_SEED), 0.1)
+        btns[s] = torch.from_numpy(b)
+        looks[s] = torch.from_numpy(l)
+    offs = [0]
+    for b, _, _ in RAGGED_GROUPS:
+        offs.append(offs[-1] + b)
+    d_btn = [btns[:, offs[g]:offs[g + 1]].contiguous().to(dev) for g in range(len(envs))]
+    d_look = [looks[:, offs[g]:offs[g + 1]].contiguous().to(dev) for g in range(len(envs))]
+
+    def run(s0, n):
+        for s in range(s0, s0 + n):
+            for g, e in enumerate(envs):
+                e.step(d_btn[g][s], d_look[g][s])
+
+    for e in envs:
+        e.reset()
+    run(0, Wm)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    run(Wm, K)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3
+    value = total * K / t
+    # e2e: actions from pinned host memory, rewards + dones back, every step
+    h_btn, h_look = btns.pin_memory(), looks.pin_memory()
+    h_rew = torch.empty((K, total), dtype=torch.float32).pin_memory()
+    h_done = torch.empty((K, total), dtype=torch.bool).pin_memory()
+    for e in envs:
+        e.reset()
+    run(0, Wm)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in range(K):
+        for g, e in enumerate(envs):
+            sl = slice(offs[g], offs[g + 1])
+            obs, rew, done = e.step(h_btn[Wm + s, sl].to(dev, non_blocking=True),
+                                    h_look[Wm + s, sl].to(dev, non_blocking=True))
+            h_rew[s, sl].copy_(rew, non_blocking=True)
+            h_done[s, sl].copy_(done, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    te = ev0.elapsed_time(ev1) / 1e3
+    line = {
+        "impl": "reference", "metric": RAGGED_METRIC, "value": value, "unit": "env-steps/s", "n_gpus": 1,
+        "steps": K, "warmup": Wm, "ms_per_step": t / K * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions seed 3)",
+        "config": {"workload": "ragged: the same 6 groups, one reference MineEnv each, stepped in turn",
+                   "global_batch": total, "trajectory": f"steps {Wm}..{Wm + K - 1} after reset()",
+                   "path": "reference src/kernels.cu launch_step_uint8 + MineEnv.step glue per group (eager)"},
+        "e2e": {"value": total * K / te, "unit": "env-steps/s", "h2d_bytes_per_step": total * 16,
+                "d2h_bytes_per_step": total * 5},
+        "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": None, "kind": "reference",
+                         "sample": f"{K} steps of all 6 groups; the reference implementation is CUDA-only, so "
+                                   "this arm runs its own kernels on the same B200"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,13 +636,15 @@ def main():
     ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,tile_w")
     ap.add_argument("--traffic-bytes", type=float, default=0.0,
                     help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
+    ap.add_argument("--workload", default="peak", choices=["peak", "ragged"],
+                    help="peak: B=32768, 16^3, 32x32 (default); ragged: 24,576 envs in 6 groups")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
-        run_reference(args)
+        run_reference_ragged(args) if args.workload == "ragged" else run_reference(args)
     else:
-        run_mine(args)
+        run_mine_ragged(args) if args.workload == "ragged" else run_mine(args)
 
 
 if __name__ == "__main__":

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MC_ABI_VERSION 1
+#define MC_ABI_VERSION 2
 
 /* status codes */
 #define MC_OK 0
@@ -111,9 +111,12 @@ typedef struct mc_env mc_env;
 /* Launch shape of the fused kernel (see mc_env_set_fused_config). */
 typedef struct mc_fused_config {
     int32_t stage;         /* 1: bulk-copy each marched world into shared memory */
-    int32_t warps_per_cta; /* 4 or 8 */
+    int32_t warps_per_cta; /* 1..8 warps per CTA */
     int32_t ctas_per_sm;   /* persistent grid = SMs x ctas_per_sm */
     int32_t tile_w;        /* a warp marches tiles of tile_w x (32/tile_w) pixels: 4, 8, 16 or 32 */
+    int32_t team_warps;    /* 1: one warp steps and renders each env (4 or 8 warps per CTA);
+                              1, 2, 4 or 8 with coop = 1: a team of that many warps renders each env */
+    int32_t coop;          /* 1: the team shares one env (its image bands and one staged world) */
 } mc_fused_config;
 
 /* ---- library ---------------------------------------------------------- */
@@ -154,6 +157,45 @@ int mc_env_get_fused_config(const mc_env* env, mc_fused_config* cfg);
 int mc_env_check_error(mc_env* env, void* stream);
 /* Bytes of dynamic shared memory the fused kernel uses per CTA. */
 int64_t mc_env_fused_smem_bytes(const mc_env* env);
+
+/* ---- ragged batches: several env handles stepped by one launch ---------
+ * No counterpart in the reference, which runs one world size and one
+ * resolution per MineEnv (minecu/__init__.py:141-212) and one kernel
+ * sequence per step.  A ragged handle borrows up to MC_RAGGED_MAX_GROUPS env
+ * handles ("groups": different world sizes, resolutions, parameters; same
+ * numerics and the same observation kind) and steps all of them with one
+ * persistent fused launch, then regenerates the worlds of each group in
+ * which an env was done, exactly as mc_env_step would.  Every group's
+ * results are identical to stepping that env handle alone with the fused
+ * form.  Actions are concatenated in group order (sum of batch sizes). */
+#define MC_RAGGED_MAX_GROUPS 16
+typedef struct mc_ragged mc_ragged;
+typedef struct mc_ragged_config {
+    int32_t warps_per_cta; /* 1..8 warps per CTA */
+    int32_t ctas_per_sm;   /* persistent grid = SMs x ctas_per_sm */
+    int32_t team_warps;    /* warps per team (1, 2, 4, 8; divides warps_per_cta) */
+    int32_t stage[MC_RAGGED_MAX_GROUPS];  /* per group: 1 = bulk-copy each marched world into shared memory */
+    int32_t tile_w[MC_RAGGED_MAX_GROUPS]; /* per group: pixel tile tile_w x (32/tile_w), 4/8/16/32 */
+    int32_t coop[MC_RAGGED_MAX_GROUPS];   /* per group: 1 = a whole team renders each env; 0 = one warp per env */
+} mc_ragged_config;
+/* The env handles must outlive the ragged handle; re-pointing one of them
+ * (mc_env_set_state) is picked up at the next step. */
+int mc_ragged_create(mc_env* const* groups, int32_t ngroups, mc_ragged** out);
+int mc_ragged_destroy(mc_ragged* r);
+int mc_ragged_set_config(mc_ragged* r, const mc_ragged_config* cfg);
+int mc_ragged_get_config(const mc_ragged* r, mc_ragged_config* cfg);
+/* Total envs over the groups, and the dynamic shared memory per CTA. */
+int64_t mc_ragged_total_envs(const mc_ragged* r);
+int64_t mc_ragged_smem_bytes(const mc_ragged* r);
+/* One step of every group: buttons int8[total,8] + look float32[total,2]. */
+int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* look, void* stream);
+/* One step of every group: discrete actions uint8[total]. */
+int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, void* stream);
+/* K steps of actions uint8[K,total] in one CUDA graph (cached per actions, K and config). */
+int mc_ragged_rollout(mc_ragged* r, const uint8_t* actions, int32_t K, void* stream);
+int mc_ragged_rollout_prepare(mc_ragged* r, const uint8_t* actions, int32_t K);
+/* Reads and clears the device error words of the launch and of every group. */
+int mc_ragged_check_error(mc_ragged* r, void* stream);
 
 /* ---- stateless kernels: the reference's _C functions ------------------ */
 /* generate_world_kernel (src/kernels.cu:1793-1828) via launch_generate_world

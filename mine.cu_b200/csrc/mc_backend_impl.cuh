@@ -118,6 +118,27 @@ __device__ __forceinline__ Dec decode_buttons(const int8_t b[8], float l0, float
     return d;
 }
 
+// Actions of one env group: discrete actions, or buttons + look.
+struct ActionSrc {
+    const uint8_t* actions;
+    const int8_t* buttons;
+    const float* look;
+};
+__device__ __forceinline__ void load_action_from(const ActionSrc& a, float look_delta, long long i, int8_t b[8],
+                                                 float& l0, float& l1) {
+    if (a.actions) {
+        float lk[2];
+        mc_discrete_to_buttons(a.actions[i], look_delta, b, lk);
+        l0 = lk[0];
+        l1 = lk[1];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) b[k] = a.buttons[i * 8 + k];
+        l0 = a.look[i * 2 + 0];
+        l1 = a.look[i * 2 + 1];
+    }
+}
+
 __device__ __forceinline__ void load_action(const mc_kp& p, long long i, int8_t b[8], float& l0, float& l1) {
     if (p.actions) {
         float lk[2];
@@ -1061,6 +1082,106 @@ __device__ __forceinline__ long long next_env(const mc_kp& p, long long cur, lon
     return (long long)__shfl_sync(0xffffffffu, v, 0);
 }
 
+// Per-warp view of the shared-memory tables and buffers used by one env.
+struct FusedCtx {
+    const float* s_u;            // per-column u of the env's image
+    const float* s_v;            // per-row v
+    const float (*s_rgb)[3];
+    const float* s_sky;
+    const uint8_t (*s_rgb8)[3];
+    const uint8_t* s_sky8;
+    uint8_t* stage;              // staging band of this warp
+    int8_t* sworld;              // staged world of this warp
+    uint32_t mbar_a;             // mbarrier of this warp
+    float rcp_vd;                // reciprocal of the env's view distance
+};
+
+// Shared colour tables: 13*3 + 4 floats, 13*3 + 3 bytes.
+constexpr int kColourTableBytes = 13 * 3 * 4 + 16 + 13 * 3 + 3;
+static_assert(kColourTableBytes <= MC_COLOUR_TABLE_BYTES, "colour tables");
+
+__device__ __forceinline__ void load_colour_tables(uint8_t* base, FusedCtx& cx) {
+    float (*s_rgb)[3] = reinterpret_cast<float (*)[3]>(base);
+    float* s_sky = reinterpret_cast<float*>(s_rgb + 13);
+    uint8_t (*s_rgb8)[3] = reinterpret_cast<uint8_t (*)[3]>(s_sky + 4);
+    uint8_t* s_sky8 = reinterpret_cast<uint8_t*>(s_rgb8 + 13);
+    for (int k = threadIdx.x; k < 39; k += blockDim.x) {
+        s_rgb[k / 3][k % 3] = c_rgb[k / 3][k % 3];
+        s_rgb8[k / 3][k % 3] = c_rgb8[k / 3][k % 3];
+    }
+    if (threadIdx.x < 3) {
+        s_sky[threadIdx.x] = c_sky[threadIdx.x];
+        s_sky8[threadIdx.x] = c_sky8[threadIdx.x];
+    }
+    cx.s_rgb = s_rgb;
+    cx.s_sky = s_sky;
+    cx.s_rgb8 = s_rgb8;
+    cx.s_sky8 = s_sky8;
+}
+
+// u/v tables of one image size (threads of the CTA cooperate).
+template <int FAM>
+__device__ __forceinline__ void build_uv_tables(const mc_kp& p, float* s_u, float* s_v) {
+    const int W = p.W, H = p.H;
+    float pb_su = 0.0f, pb_sv = 0.0f;
+    if (FAM == MC_FAM_PREBASIS) prebasis_scales(W, H, p.fov, &pb_su, &pb_sv);
+    for (int k = threadIdx.x; k < W; k += blockDim.x) {
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) s_u[k] = u_shaded(k, W, H, p.fov);
+        else if (FAM == MC_FAM_MINIMAL || FAM == MC_FAM_FP16) s_u[k] = u_minimal(k, W, H, p.fov);
+        else s_u[k] = u_prebasis(k, W, pb_su);
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) s_v[k] = v_shaded(k, H, p.fov);
+        else if (FAM == MC_FAM_MINIMAL || FAM == MC_FAM_FP16) s_v[k] = v_minimal(k, H, p.fov);
+        else s_v[k] = v_prebasis(k, H, pb_sv);
+    }
+}
+
+// The parameters a ray needs.
+struct RayPar {
+    int wx, wy, wz, max_steps, gh;
+    float vd;
+};
+__device__ __forceinline__ RayPar ray_par(const mc_kp& p) {
+    RayPar r;
+    r.wx = p.wx;
+    r.wy = p.wy;
+    r.wz = p.wz;
+    r.max_steps = p.max_steps;
+    r.gh = p.gh;
+    r.vd = p.vd;
+    return r;
+}
+
+// One pixel's ray through one of the two voxel sources.
+template <int FAM, class V>
+__device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const Dda0& d0, float u, float v,
+                                           const V& vox, bool inside, bool skip_first) {
+    if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST)
+        return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
+                                                    inside, skip_first);
+    if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
+    return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first);
+}
+
+__device__ __forceinline__ void mbar_init_warp(uint32_t mbar_a, int lane) {
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+}
+
+// Last warp of a dynamically scheduled launch resets the work counters.
+__device__ __forceinline__ void finish_dynamic(int32_t* flags, long long total_warps) {
+    __threadfence();
+    unsigned prev = atomicAdd(reinterpret_cast<unsigned*>(&flags[MC_FLAG_WARPS_DONE]), 1u);
+    if (prev == (unsigned)(total_warps - 1)) {
+        flags[MC_FLAG_WORK] = 0;
+        flags[MC_FLAG_WARPS_DONE] = 0;
+        __threadfence();
+    }
+}
+
 #ifndef MC_FUSED_MIN_BLOCKS
 #define MC_FUSED_MIN_BLOCKS 4
 #endif
@@ -1350,6 +1471,404 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Team kernel: env groups of any size, stepped by teams of warps
+// ---------------------------------------------------------------------------
+// A CTA of warps_per_cta warps is split into teams of team_warps warps.  A
+// team claims one work unit at a time from a device counter:
+//  * a cooperative group's unit is ONE env: the team's first warp steps the
+//    agent, then all warps of the team march row bands of its image (bands
+//    claimed from a shared counter), reading the world from one shared-memory
+//    copy per team when staged.  Big images over big worlds then keep an
+//    SM's L1 and shared memory on few worlds, like a per-pixel kernel;
+//  * a per-warp group's unit is team_warps envs, one per warp, each stepped
+//    and rendered by its warp alone.
+// Units are ordered by decreasing per-env cost across groups, so the most
+// expensive envs are claimed first and do not straggle at the end.
+
+// What the render of one env needs from its agent step.
+struct EnvRender {
+    Cam c;
+    int bits;      // MC_ER_*
+    int fill_blk;  // block of the uniform fill of a buried camera
+    int mod_idx;   // voxel index the interaction wrote, -1 if none
+    int mod_val;
+};
+enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
+
+struct TeamShared {
+    unsigned unit[2];  // claimed units, alternating slots
+    int band_ctr;      // next row band of the cooperative env
+    int pad;
+    EnvRender r;       // the cooperative env
+};
+static_assert(sizeof(TeamShared) <= MC_TEAM_HEAD_BYTES, "team head");
+
+// Decode, episode rule, physics, interaction, reset, counters and camera of
+// env e, run by one whole warp: every lane computes the same values, lane 0
+// writes the state.
+template <int FAM>
+__device__ __forceinline__ EnvRender agent_step(const mc_kp& p, const ActionSrc& act, long long e, int lane) {
+    const int wxz = p.wx * p.wz;
+    const int wxyz = wxz * p.wy;
+    int8_t btn[8];
+    float l0, l1;
+    load_action_from(act, p.look_delta, e, btn, l0, l1);
+    Dec d = decode_buttons(btn, l0, l1, p.sprint_mult);
+    int32_t cnt = p.ext_done ? 0 : p.step_count[e];
+    bool done = p.ext_done ? (p.do_reset[e] != 0) : episode_done(p, cnt);
+    Agent a = load_agent(p, e);
+    physics(a, d, p);
+    int8_t* gw = p.voxels + e * (long long)wxyz;
+    float reward;
+    int8_t mod_val;
+    int mod_idx = interact_warp(gw, a, d.brk, d.place, p, lane, &reward, &mod_val);
+    if (done) reset_agent(a, p);
+    if (lane == 0) {
+        store_agent(p, e, a);
+        if (!p.ext_done) {
+            p.step_count[e] = done ? 1 : cnt + 1;
+            p.do_reset[e] = done ? 1 : 0;
+        }
+        p.rewards[e] = reward;
+        p.cameras[e * 5 + 0] = a.x;
+        p.cameras[e * 5 + 1] = a.y;
+        p.cameras[e * 5 + 2] = a.z;
+        p.cameras[e * 5 + 3] = a.yaw;
+        p.cameras[e * 5 + 4] = a.pitch;
+        if (p.dbg_interact) p.dbg_interact[e] = mod_idx;
+    }
+    EnvRender r;
+    if (FAM == MC_FAM_PREBASIS) {
+        float bas[13];
+        basis_compute(a.x, a.y, a.z, a.yaw, a.pitch, p.W, p.H, p.fov, bas);
+        r.c = cam_from_basis(bas);
+        if (p.basis && lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 13; ++k) p.basis[e * 14 + k] = bas[k];
+        }
+    } else {
+        r.c = cam_trig(a.x, a.y, a.z, a.yaw, a.pitch);
+    }
+    // Every ray starts in the eye's voxel.  If the first DDA step already
+    // hits (the eye is inside a solid voxel, or below ground for the
+    // ground-shortcut family), every pixel of the env gets the same colour.
+    const Cam& c = r.c;
+    const int ex = (int)floorf(c.eye_x), ey = (int)floorf(c.eye_y), ez = (int)floorf(c.eye_z);
+    bool eye_inb = (unsigned)ex < (unsigned)p.wx && (unsigned)ey < (unsigned)p.wy && (unsigned)ez < (unsigned)p.wz;
+    int8_t eye_blk = AIR;
+    __syncwarp();
+    if (eye_inb) eye_blk = gw[ey * wxz + ex * p.wz + ez];
+    bool inside = false, buried, skip_first;
+    int fill_blk = eye_blk;
+    if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+        inside = eye_inside(c, p.wx, p.wy, p.wz, p.vd);
+        bool start_hit = eye_blk >= 0;
+        if (FAM == MC_FAM_SHADED_FAST && ey < p.gh) {
+            start_hit = true;
+            fill_blk = (ey == p.gh - 1) ? GRASS : DIRT;
+        }
+        buried = inside && p.vd > 0.0f && p.max_steps > 0 && start_hit;
+        // not buried: the first DDA step of every ray tests the eye voxel
+        // and advances; when that test is known to fail, rays start advanced
+        skip_first = inside && p.vd > 0.0f && p.max_steps > 0 && eye_blk < 0 &&
+                     !(FAM == MC_FAM_SHADED_FAST && ey < p.gh);
+    } else {
+        buried = p.max_steps > 0 && eye_inb && eye_blk >= 0;
+        skip_first = p.max_steps > 0 && !(eye_inb && eye_blk >= 0);
+    }
+    r.bits = (done ? MC_ER_DONE : 0) | (buried ? MC_ER_BURIED : 0) | (inside ? MC_ER_INSIDE : 0) |
+             (skip_first ? MC_ER_SKIP : 0);
+    r.fill_blk = fill_blk;
+    r.mod_idx = mod_idx;
+    r.mod_val = mod_val;
+    return r;
+}
+
+// Repeating 48-byte pattern written with 16-byte stores by nt threads.
+__device__ __forceinline__ void fill_pattern16_n(uint8_t* dst, int bytes, uint4 p0, uint4 p1, uint4 p2, int t,
+                                                 int nt) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    const int n = bytes >> 4, adv = nt % 3;
+    int m = t % 3;
+    for (int k = t; k < n; k += nt) {
+        d[k] = (m == 0) ? p0 : ((m == 1) ? p1 : p2);
+        m += adv;
+        if (m >= 3) m -= 3;
+    }
+}
+
+// The uniform observation of a buried camera, written by nt threads.
+template <int FAM, bool F32>
+__device__ __forceinline__ void fill_env(const mc_kp& p, long long e, const EnvRender& r, const FusedCtx& cx, int t,
+                                         int nt) {
+    const int HW = p.W * p.H;
+    const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
+    uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
+    const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
+    Hit h;
+    h.blk = r.fill_blk;
+    h.face = -1;
+    h.t = 0.0f;
+    h.step_y = 1;
+    uint8_t bytes[12];
+    if (F32 || FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+        float rgb[3];
+        shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, cx.rcp_vd,
+                                                                                              cx.s_rgb, cx.s_sky, rgb);
+        if (F32) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                uint32_t w32 = __float_as_uint(rgb[k]);
+                bytes[4 * k + 0] = (uint8_t)(w32);
+                bytes[4 * k + 1] = (uint8_t)(w32 >> 8);
+                bytes[4 * k + 2] = (uint8_t)(w32 >> 16);
+                bytes[4 * k + 3] = (uint8_t)(w32 >> 24);
+            }
+        } else {
+            bytes[0] = (uint8_t)to_u8(rgb[0]);
+            bytes[1] = (uint8_t)to_u8(rgb[1]);
+            bytes[2] = (uint8_t)to_u8(rgb[2]);
+        }
+    } else {
+        bytes[0] = cx.s_rgb8[r.fill_blk][0];
+        bytes[1] = cx.s_rgb8[r.fill_blk][1];
+        bytes[2] = cx.s_rgb8[r.fill_blk][2];
+    }
+    const int period = F32 ? 12 : 3;
+    if (vec_ok) {
+        uint32_t w[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            w[k] = (uint32_t)bytes[(4 * k + 0) % period] | ((uint32_t)bytes[(4 * k + 1) % period] << 8) |
+                   ((uint32_t)bytes[(4 * k + 2) % period] << 16) | ((uint32_t)bytes[(4 * k + 3) % period] << 24);
+        }
+        fill_pattern16_n(oenv, (int)obs_env_bytes, make_uint4(w[0], w[1], w[2], w[3]),
+                         make_uint4(w[4], w[5], w[6], w[7]), make_uint4(w[8], w[9], w[10], w[11]), t, nt);
+    } else {
+        for (long long k = t; k < obs_env_bytes; k += nt) oenv[k] = bytes[k % period];
+    }
+    if (p.dbg_pixel) {
+        int16_t code = dbg_code(h);
+        for (int k = t; k < HW; k += nt) p.dbg_pixel[e * HW + k] = code;
+    }
+}
+
+// March row bands of env e's image with one warp: every band when band_ctr is
+// null, else the bands this warp claims from the team's shared counter.
+template <int FAM, bool F32, class V>
+__device__ __forceinline__ void render_env(const mc_kp& p, long long e, const EnvRender& r, const FusedCtx& cx,
+                                           const V& vox, int tile_w, int lane, int* band_ctr) {
+    // parameters in registers: p may live in shared memory, which the band
+    // stores below would otherwise force to be re-read per pixel
+    const int W = p.W, H = p.H;
+    const RayPar rp = ray_par(p);
+    int16_t* const dbg_pixel = p.dbg_pixel;
+    const float vd = p.vd;
+    const long long obs_env_bytes = (long long)W * H * 3 * (F32 ? 4 : 1);
+    uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
+    const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
+    const bool inside = (r.bits & MC_ER_INSIDE) != 0, skip_first = (r.bits & MC_ER_SKIP) != 0;
+    const Dda0 d0 = dda0(r.c);
+    const int TW = tile_w, TH = 32 / tile_w;
+    const int lx = lane % TW, ly = lane / TW;
+    const int bpp = 3 * (F32 ? 4 : 1);
+    const int nbands = (H + TH - 1) / TH;
+    auto claim = [&]() -> int {
+        int v = 0;
+        if (lane == 0) v = atomicAdd(band_ctr, 1);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    for (int b = band_ctr ? claim() : 0; b < nbands; b = band_ctr ? claim() : b + 1) {
+        const int row0 = b * TH;
+        const int py = row0 + ly;
+        const float v = (py < H) ? cx.s_v[py] : 0.0f;
+        for (int tx0 = 0; tx0 < W; tx0 += TW) {
+            const int px = tx0 + lx;
+            if (px < W && py < H) {
+                const float u = cx.s_u[px];
+                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first);
+                const int so = ly * W + px;  // pixel within the staged band
+                if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+                    float rgb[3];
+                    shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
+                        h, vd, cx.rcp_vd, cx.s_rgb, cx.s_sky, rgb);
+                    if (F32) {
+                        float* sf = reinterpret_cast<float*>(cx.stage) + so * 3;
+                        sf[0] = rgb[0];
+                        sf[1] = rgb[1];
+                        sf[2] = rgb[2];
+                    } else {
+                        uint8_t* sb = cx.stage + so * 3;
+                        sb[0] = (uint8_t)to_u8(rgb[0]);
+                        sb[1] = (uint8_t)to_u8(rgb[1]);
+                        sb[2] = (uint8_t)to_u8(rgb[2]);
+                    }
+                } else {
+                    const uint8_t* col = (h.blk >= 0) ? cx.s_rgb8[h.blk] : cx.s_sky8;
+                    uint8_t* sb = cx.stage + so * 3;
+                    sb[0] = col[0];
+                    sb[1] = col[1];
+                    sb[2] = col[2];
+                }
+                if (dbg_pixel) dbg_pixel[e * W * H + py * W + px] = dbg_code(h);
+            }
+        }
+        __syncwarp();
+        // copy the band (rows row0 .. row0+TH-1) out
+        const int nbytes = min(TH, H - row0) * W * bpp;
+        uint8_t* dst = oenv + (long long)row0 * W * bpp;
+        if (vec_ok && (nbytes & 15) == 0 && (((long long)row0 * W * bpp) & 15) == 0) {
+            const uint4* s4 = reinterpret_cast<const uint4*>(cx.stage);
+            uint4* d4 = reinterpret_cast<uint4*>(dst);
+            for (int k = lane; k < (nbytes >> 4); k += 32) d4[k] = s4[k];
+        } else {
+            for (int k = lane; k < nbytes; k += 32) dst[k] = cx.stage[k];
+        }
+        __syncwarp();
+    }
+}
+
+// Bulk copy of one world into shared memory, waited for with a bound.
+__device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, int8_t* dst, const int8_t* src,
+                                            int bytes, int lane) {
+    if (lane == 0) {
+        // generic-proxy reads of the previous world must precede the copy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_a), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(dst)),
+            "l"(src), "r"(bytes), "r"(mbar_a)
+            : "memory");
+    }
+    const bool ok = mbar_wait(mbar_a, phase);
+    phase ^= 1u;
+    return ok;
+}
+
+__device__ __forceinline__ void team_sync(int bar, int nthreads) {
+    if (nthreads == 32)
+        __syncwarp();
+    else
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+}
+
+#ifndef MC_TEAM_MIN_BLOCKS
+#define MC_TEAM_MIN_BLOCKS 3  // 80 registers: the render path without spills
+#endif
+template <int FAM, bool F32>
+__global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __grid_constant__ mc_ragged_kp rk) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int TWN = rk.team_warps;
+    const int team = warp / TWN, wt = warp % TWN;
+    const int teams_per_cta = nwarps / TWN;
+    const int G = rk.ngroups;
+    // layout: colour tables | u/v tables | teams | warps; the groups'
+    // parameter blocks stay in the kernel's parameter space
+    FusedCtx cx;
+    load_colour_tables(smem, cx);
+    float* tables = reinterpret_cast<float*>(smem + rk.tables_off);
+    for (int g = 0; g < G; ++g)
+        build_uv_tables<FAM>(rk.groups[g], tables + rk.uv_off[g], tables + rk.uv_off[g] + rk.groups[g].W);
+    TeamShared* ts = reinterpret_cast<TeamShared*>(smem + rk.teams_off + team * rk.team_bytes);
+    int8_t* tworld = reinterpret_cast<int8_t*>(ts) + MC_TEAM_HEAD_BYTES;
+    uint8_t* wbase = smem + rk.warps_off + warp * rk.warp_bytes;
+    cx.mbar_a = smem_u32(wbase);
+    cx.stage = wbase + 16;
+    if (rk.stage_mask) mbar_init_warp(cx.mbar_a, lane);
+    const bool claimer = (wt == 0 && lane == 0);
+    const long long total_teams = (long long)gridDim.x * teams_per_cta;
+    const long long my_team = (long long)blockIdx.x * teams_per_cta + team;
+    const unsigned total_units = (unsigned)rk.ustart[G];
+    auto claim = [&](int k) -> unsigned {
+        if (rk.sched_dynamic) return atomicAdd(reinterpret_cast<unsigned*>(&rk.flags[MC_FLAG_WORK]), 1u);
+        const long long u = my_team + (long long)k * total_teams;
+        return u < (long long)total_units ? (unsigned)u : total_units;
+    };
+    if (claimer) ts->unit[0] = claim(0);
+    __syncthreads();
+    const int bar = 1 + team, nthr = TWN * 32;
+    uint32_t phase = 0;
+    unsigned done_groups = 0;
+    bool warp_no_stage = false;
+    for (int k = 0;; ++k) {
+        const unsigned u = ts->unit[k & 1];
+        if (u >= total_units) break;
+        int vg = 0;
+        while (vg + 1 < G && (long long)u >= rk.ustart[vg + 1]) ++vg;
+        const int g = rk.order[vg];
+        const mc_kp& p = rk.groups[g];
+        cx.s_u = tables + rk.uv_off[g];
+        cx.s_v = cx.s_u + p.W;
+        cx.rcp_vd = N::rcp_of(p.vd);
+        const long long local = (long long)u - rk.ustart[vg];
+        const int wxyz = p.wx * p.wy * p.wz;
+        const bool coop = (rk.coop_mask >> g) & 1;
+        // coop: warp 0 steps the env and the team renders it; else each warp
+        // steps and renders its own env of the unit
+        const long long e = coop ? local : local * TWN + wt;
+        const bool stepper = coop ? (wt == 0) : (e < p.B);
+        const int8_t* gw = p.voxels + e * (long long)wxyz;
+        int8_t* world = coop ? tworld : tworld + wt * rk.slot_bytes;
+        EnvRender r;
+        bool staged = false;
+        if (stepper) {
+            const long long s0 = rk.start[g];
+            const ActionSrc act{rk.actions ? rk.actions + s0 : nullptr, rk.actions ? nullptr : rk.buttons + 8 * s0,
+                                rk.actions ? nullptr : rk.look + 2 * s0};
+            r = agent_step<FAM>(p, act, e, lane);
+            if (lane == 0) {
+                if (r.bits & MC_ER_DONE) done_groups |= 1u << g;
+                if (rk.rewards_cat) {
+                    rk.rewards_cat[rk.start[g] + e] = p.rewards[e];
+                    rk.dones_cat[rk.start[g] + e] = (uint8_t)(r.bits & MC_ER_DONE);
+                }
+            }
+            staged = ((rk.stage_mask >> g) & 1) && !(r.bits & MC_ER_BURIED) && !warp_no_stage;
+            if (staged) {
+                if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane)) {
+                    // the interaction may have written after the copy read the byte
+                    if (lane == 0 && r.mod_idx >= 0) world[r.mod_idx] = (int8_t)r.mod_val;
+                } else {
+                    if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
+                    warp_no_stage = true;  // the copy may still land: render from global memory from now on
+                    staged = false;
+                }
+            }
+            if (coop && lane == 0) {
+                r.bits |= staged ? MC_ER_STAGED : 0;
+                ts->r = r;
+                ts->band_ctr = 0;
+            }
+            __syncwarp();
+        }
+        if (coop) {
+            team_sync(bar, nthr);
+            r = ts->r;
+            staged = (r.bits & MC_ER_STAGED) != 0;
+        }
+        if (coop || stepper) {
+            if (r.bits & MC_ER_BURIED)
+                fill_env<FAM, F32>(p, e, r, cx, coop ? wt * 32 + lane : lane, coop ? nthr : 32);
+            else
+                render_env<FAM, F32>(p, e, r, cx, VoxGlobal{staged ? world : gw}, rk.tile_w[g], lane,
+                                     coop ? &ts->band_ctr : nullptr);
+        }
+        if (claimer) ts->unit[(k + 1) & 1] = claim(k + 1);
+        team_sync(bar, nthr);
+    }
+    if (lane == 0) {
+        for (int g = 0; g < G; ++g)
+            if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);
+    }
+    if (claimer && rk.sched_dynamic) finish_dynamic(rk.flags, total_teams);
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -1429,6 +1948,40 @@ template <int FAM, bool F32>
 static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
     return cfg->stage ? launch_fused_t<FAM, F32, true>(p, cfg, num_sms, s)
                       : launch_fused_t<FAM, F32, false>(p, cfg, num_sms, s);
+}
+
+template <int FAM, bool F32>
+static int launch_team_t(const mc_ragged_kp* rk, int warps_per_cta, int ctas_per_sm, int num_sms, cudaStream_t s) {
+    auto kern = k_step_team<FAM, F32>;
+    size_t smem = (size_t)rk->warps_off + (size_t)warps_per_cta * rk->warp_bytes;
+    static size_t attr_set = 0;
+    if (smem > 48 * 1024 && smem > attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        attr_set = smem;
+    }
+    const int teams_per_cta = warps_per_cta / rk->team_warps;
+    long long ctas_needed = (rk->ustart[rk->ngroups] + teams_per_cta - 1) / teams_per_cta;
+    long long grid = (long long)num_sms * (ctas_per_sm > 0 ? ctas_per_sm : 1);
+    if (grid > ctas_needed) grid = ctas_needed;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, 32 * warps_per_cta, smem, s>>>(*rk);
+    return (int)cudaGetLastError();
+}
+
+static int step_team(const mc_ragged_kp* rk, int family, int obs_f32, int warps_per_cta, int ctas_per_sm,
+                     int num_sms, cudaStream_t s) {
+    if (rk->ustart[rk->ngroups] == 0) return 0;
+    switch (family) {
+        case MC_FAM_SHADED:
+            return obs_f32 ? launch_team_t<MC_FAM_SHADED, true>(rk, warps_per_cta, ctas_per_sm, num_sms, s)
+                           : launch_team_t<MC_FAM_SHADED, false>(rk, warps_per_cta, ctas_per_sm, num_sms, s);
+        case MC_FAM_SHADED_FAST: return launch_team_t<MC_FAM_SHADED_FAST, false>(rk, warps_per_cta, ctas_per_sm, num_sms, s);
+        case MC_FAM_MINIMAL: return launch_team_t<MC_FAM_MINIMAL, false>(rk, warps_per_cta, ctas_per_sm, num_sms, s);
+        case MC_FAM_FP16: return launch_team_t<MC_FAM_FP16, false>(rk, warps_per_cta, ctas_per_sm, num_sms, s);
+        case MC_FAM_PREBASIS: return launch_team_t<MC_FAM_PREBASIS, false>(rk, warps_per_cta, ctas_per_sm, num_sms, s);
+        default: return (int)cudaErrorInvalidValue;
+    }
 }
 
 static int step_fused(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {

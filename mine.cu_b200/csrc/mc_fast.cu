@@ -19,6 +19,7 @@ static const mc_backend g_backend = {
     interact_launch,
     coalesced_launch,
     fused_smem,
+    step_team,
 };
 }  // namespace mc_fast
 

@@ -83,7 +83,43 @@ struct mc_fused_cfg {
     int stage;          // 1: copy each rendered world into shared memory with a bulk copy; 0: read voxels from L1/L2
     int warps_per_cta;  // 4 or 8
     int ctas_per_sm;    // persistent grid = SMs * ctas_per_sm
-    int tile_w;         // march tiles of tile_w x (32/tile_w) pixels (8, 16 or 32)
+    int tile_w;         // march tiles of tile_w x (32/tile_w) pixels (4, 8, 16 or 32)
+    int team_warps;     // 1 with coop = 0: the per-warp kernel; else the team kernel with teams of this many warps
+    int coop;           // team kernel: 1 = a team renders each env together
+};
+
+// Several env groups stepped by one launch of the team kernel (k_step_team).
+enum { MC_MAX_GROUPS = 16 };
+enum { MC_COLOUR_TABLE_BYTES = 224 };  // shared colour tables of the fused kernels (16-aligned)
+enum { MC_TEAM_HEAD_BYTES = 128 };     // per-team shared words ahead of the team's world buffer
+struct mc_ragged_kp {
+    mc_kp groups[MC_MAX_GROUPS];    // the groups' parameter blocks (kernel parameter space)
+    // optional: every env's reward and done flag also written at its global
+    // index (one contiguous read-back for a batch of jobs)
+    float* rewards_cat;
+    uint8_t* dones_cat;
+    // actions of all groups, concatenated in group order: discrete actions, or buttons + look
+    const uint8_t* actions;
+    const int8_t* buttons;
+    const float* look;
+    int32_t* flags;                      // work counter of the launch
+    long long start[MC_MAX_GROUPS + 1];  // first global env index of each group; start[ngroups] = total
+    int ngroups;
+    // work units: groups visited in `order` (most expensive envs first);
+    // ustart[v] = first unit of the v-th visited group, ustart[ngroups] = total units
+    int order[MC_MAX_GROUPS];
+    long long ustart[MC_MAX_GROUPS + 1];
+    int team_warps;                 // warps per team
+    int coop_mask;                  // bit g: a whole team renders each env of group g
+    int stage_mask;                 // bit g: group g's worlds are bulk-copied into shared memory
+    int tile_w[MC_MAX_GROUPS];
+    int uv_off[MC_MAX_GROUPS];      // float offset of each group's u table (v follows)
+    int sched_dynamic;              // 1: teams claim units from flags[MC_FLAG_WORK]
+    // shared-memory layout (bytes): colour tables at 0, then
+    int tables_off, teams_off, warps_off;
+    int team_bytes;                 // MC_TEAM_HEAD_BYTES + the team's world buffer
+    int slot_bytes;                 // world slot of one warp of a per-warp staged group
+    int warp_bytes;                 // 16 (mbarrier) + one band of observation bytes
 };
 
 // One numerics back end (ref_fast or ieee).
@@ -101,6 +137,9 @@ struct mc_backend {
     int (*render_coalesced)(const int8_t* vox_yxzb, const float* basis, uint8_t* out, int B, int ws,
                             int W, int H, int max_steps, cudaStream_t s);
     size_t (*fused_smem_bytes)(const mc_kp* p, const mc_fused_cfg* cfg);
+    // the team kernel over rk's groups: grid = SMs x ctas_per_sm (at most one unit per team)
+    int (*step_team)(const mc_ragged_kp* rk, int family, int obs_f32, int warps_per_cta, int ctas_per_sm,
+                     int num_sms, cudaStream_t s);
 };
 
 extern "C" const mc_backend* mc_backend_fast();

@@ -14,6 +14,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -408,6 +409,97 @@ static bool dones_possible(const mc_kp& k) {
     return k.episode_length > 0;
 }
 
+static inline int align16i(long long x) { return (int)((x + 15) & ~15LL); }
+
+// Launch description of the team kernel over G groups (host copies of their
+// parameter blocks, copied into the launch's parameter block); flags and
+// actions are left to the caller.
+static void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
+                        int team_warps, int warps_per_cta, mc_ragged_kp* rk) {
+    *rk = mc_ragged_kp{};
+    rk->ngroups = G;
+    rk->team_warps = team_warps;
+    rk->sched_dynamic = 1;
+    const int bpp = 3 * (kps[0]->obs_f32 ? 4 : 1);
+    long long start = 0;
+    int uv = 0, band = 16, coop_world = 0, slot = 0;
+    for (int g = 0; g < G; ++g) {
+        const mc_kp& k = *kps[g];
+        const long long wxyz = (long long)k.wx * k.wy * k.wz;
+        rk->groups[g] = k;
+        rk->start[g] = start;
+        start += k.B;
+        rk->uv_off[g] = uv;
+        uv += k.W + k.H;
+        rk->tile_w[g] = tile_w[g];
+        band = std::max(band, align16i((long long)k.W * (32 / tile_w[g]) * bpp));
+        if (coop[g]) rk->coop_mask |= 1 << g;
+        if (stage[g]) {
+            rk->stage_mask |= 1 << g;
+            if (coop[g])
+                coop_world = std::max(coop_world, align16i(wxyz));
+            else
+                slot = std::max(slot, align16i(wxyz));
+        }
+    }
+    rk->start[G] = start;
+    // visit the groups with the most expensive envs first (pixels x world extent)
+    std::vector<int> order(G);
+    for (int g = 0; g < G; ++g) order[g] = g;
+    auto cost = [&](int g) {
+        const mc_kp& k = *kps[g];
+        return (double)k.W * k.H * (k.wx + k.wy + k.wz);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    rk->ustart[0] = 0;
+    for (int v = 0; v < G; ++v) {
+        const int g = order[v];
+        rk->order[v] = g;
+        const long long B = kps[g]->B;
+        rk->ustart[v + 1] = rk->ustart[v] + (coop[g] ? B : (B + team_warps - 1) / team_warps);
+    }
+    rk->slot_bytes = slot;
+    rk->tables_off = MC_COLOUR_TABLE_BYTES;
+    rk->teams_off = rk->tables_off + align16i((long long)uv * 4);
+    rk->team_bytes = MC_TEAM_HEAD_BYTES + std::max(coop_world, team_warps * slot);
+    rk->warps_off = rk->teams_off + (warps_per_cta / team_warps) * rk->team_bytes;
+    rk->warp_bytes = 16 + band;
+}
+
+static long long team_smem(const mc_ragged_kp& rk, int warps_per_cta) {
+    return (long long)rk.warps_off + (long long)warps_per_cta * rk.warp_bytes;
+}
+
+static int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
+                         int team_warps, int warps_per_cta, int ctas_per_sm) {
+    if (warps_per_cta < 1 || warps_per_cta > 8) return fail(MC_ERR_INVALID, "warps_per_cta must be 1..8");
+    if (team_warps != 1 && team_warps != 2 && team_warps != 4 && team_warps != 8)
+        return fail(MC_ERR_INVALID, "team_warps must be 1, 2, 4 or 8");
+    if (warps_per_cta % team_warps) return fail(MC_ERR_INVALID, "team_warps must divide warps_per_cta");
+    if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(MC_ERR_INVALID, "ctas_per_sm out of range");
+    for (int g = 0; g < G; ++g) {
+        const int tw = tile_w[g];
+        if (tw != 4 && tw != 8 && tw != 16 && tw != 32)
+            return fail(MC_ERR_INVALID, "group %d: tile_w must be 4, 8, 16 or 32", g);
+        if ((stage[g] != 0 && stage[g] != 1) || (coop[g] != 0 && coop[g] != 1))
+            return fail(MC_ERR_INVALID, "group %d: stage and coop must be 0 or 1", g);
+        if (stage[g]) {
+            const mc_kp& k = *kps[g];
+            if (((long long)k.wx * k.wy * k.wz) & 15)
+                return fail(MC_ERR_INVALID, "group %d: stage needs world bytes %% 16 == 0", g);
+            if (((uintptr_t)k.voxels) & 15) return fail(MC_ERR_INVALID, "group %d: stage needs 16-byte aligned voxels", g);
+        }
+    }
+    mc_ragged_kp rk;
+    team_layout(kps, G, stage, tile_w, coop, team_warps, warps_per_cta, &rk);
+    if (rk.ustart[G] >= (1LL << 31)) return fail(MC_ERR_INVALID, "more than 2^31 work units");
+    const long long smem = team_smem(rk, warps_per_cta);
+    if (smem > 227 * 1024) return fail(MC_ERR_INVALID, "team kernel shared memory %lld > 227 KB", smem);
+    return MC_OK;
+}
+
+static bool team_mode(const mc_fused_cfg& f) { return f.team_warps > 1 || f.coop; }
+
 static void default_fused(mc_env* e) {
     // Staging a world in shared memory pays when it is small; the autotuner
     // (minecu/autotune.py) refines this per configuration.
@@ -415,10 +507,18 @@ static void default_fused(mc_env* e) {
     e->fcfg.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
     e->fcfg.warps_per_cta = 8;
     e->fcfg.ctas_per_sm = 4;
-    e->fcfg.tile_w = 8;
+    e->fcfg.tile_w = 4;
+    e->fcfg.team_warps = 1;
+    e->fcfg.coop = 0;
 }
 
 static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
+    if (team_mode(*f)) {
+        const mc_kp* kps[1] = {&e->kp};
+        return team_validate(kps, 1, &f->stage, &f->tile_w, &f->coop, f->team_warps, f->warps_per_cta,
+                             f->ctas_per_sm);
+    }
+    if (f->team_warps != 1) return fail(MC_ERR_INVALID, "team_warps must be 1 without coop");
     if (f->warps_per_cta != 4 && f->warps_per_cta != 8)
         return fail(MC_ERR_INVALID, "warps_per_cta must be 4 or 8");
     if (f->tile_w != 4 && f->tile_w != 8 && f->tile_w != 16 && f->tile_w != 32)
@@ -573,6 +673,17 @@ static int do_step(mc_env* e, const int8_t* buttons, const float* look, const ui
         k.look = look;
         k.actions = actions;
         rc = backend_rc(e->be->step_plain(&k, s), "step_plain");
+    } else if (form == MC_FORM_FUSED && team_mode(e->fcfg)) {
+        const mc_fused_cfg& f = e->fcfg;
+        const mc_kp* kps[1] = {&e->kp};
+        mc_ragged_kp rk;
+        team_layout(kps, 1, &f.stage, &f.tile_w, &f.coop, f.team_warps, f.warps_per_cta, &rk);
+        rk.flags = e->flags;
+        rk.actions = actions;
+        rk.buttons = buttons;
+        rk.look = look;
+        rc = backend_rc(e->be->step_team(&rk, k.family, k.obs_f32, f.warps_per_cta, f.ctas_per_sm, e->num_sms, s),
+                        "step_team");
     } else if (form == MC_FORM_FUSED) {
         rc = backend_rc(e->be->step_fused(&k, &e->fcfg, e->num_sms, s), "step_fused");
     } else {
@@ -603,7 +714,7 @@ extern "C" int mc_env_render(mc_env* e, void* stream) {
 
 static bool same_fcfg(const mc_fused_cfg& a, const mc_fused_cfg& b) {
     return a.stage == b.stage && a.warps_per_cta == b.warps_per_cta && a.ctas_per_sm == b.ctas_per_sm &&
-           a.tile_w == b.tile_w;
+           a.tile_w == b.tile_w && a.team_warps == b.team_warps && a.coop == b.coop;
 }
 
 static int rollout_graph(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
@@ -687,7 +798,7 @@ extern "C" int mc_env_rollout(mc_env* e, const uint8_t* actions, int32_t K, floa
 
 extern "C" int mc_env_set_fused_config(mc_env* e, const mc_fused_config* c) {
     if (!e || !c) return fail(MC_ERR_INVALID, "NULL argument");
-    mc_fused_cfg f{c->stage, c->warps_per_cta, c->ctas_per_sm, c->tile_w};
+    mc_fused_cfg f{c->stage, c->warps_per_cta, c->ctas_per_sm, c->tile_w, c->team_warps, c->coop};
     int rc = validate_fused(e, &f);
     if (rc) return rc;
     e->fcfg = f;
@@ -700,11 +811,20 @@ extern "C" int mc_env_get_fused_config(const mc_env* e, mc_fused_config* c) {
     c->warps_per_cta = e->fcfg.warps_per_cta;
     c->ctas_per_sm = e->fcfg.ctas_per_sm;
     c->tile_w = e->fcfg.tile_w;
+    c->team_warps = e->fcfg.team_warps;
+    c->coop = e->fcfg.coop;
     return MC_OK;
 }
 
 extern "C" int64_t mc_env_fused_smem_bytes(const mc_env* e) {
     if (!e) return -1;
+    if (team_mode(e->fcfg)) {
+        const mc_fused_cfg& f = e->fcfg;
+        const mc_kp* kps[1] = {&e->kp};
+        mc_ragged_kp rk;
+        team_layout(kps, 1, &f.stage, &f.tile_w, &f.coop, f.team_warps, f.warps_per_cta, &rk);
+        return team_smem(rk, f.warps_per_cta);
+    }
     mc_kp k = e->kp;
     return (int64_t)e->be->fused_smem_bytes(&k, &e->fcfg);
 }
@@ -722,6 +842,278 @@ extern "C" int mc_env_check_error(mc_env* e, void* stream) {
         MC_CK(cudaStreamSynchronize(s));
         return fail(MC_ERR_KERNEL, "kernel error %d (%s)", code,
                     code == MC_KERR_TMA_TIMEOUT ? "bulk copy wait timed out" : "unknown");
+    }
+    return MC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ragged handle: several env handles stepped by one launch
+// ---------------------------------------------------------------------------
+struct RaggedGraph {
+    cudaGraphExec_t exec = nullptr;
+    const uint8_t* actions = nullptr;
+    int K = 0;
+    long long version = 0;  // config/kp version it was captured with
+};
+
+static_assert(MC_RAGGED_MAX_GROUPS == MC_MAX_GROUPS, "group limit");
+
+struct mc_ragged {
+    std::vector<mc_env*> envs;  // borrowed
+    const mc_backend* be = nullptr;
+    int family = 0, obs_f32 = 0;
+    int device = 0, num_sms = 0;
+    mc_ragged_config cfg{};
+    std::vector<mc_kp> uploaded;  // group parameter blocks the cached graphs were captured with
+    int32_t* flags = nullptr;     // the launch's work counter
+    mc_ragged_kp rk{};
+    long long version = 1;
+    cudaStream_t cap_stream = nullptr;
+    std::vector<RaggedGraph> graphs;
+};
+
+static long long ragged_wxyz(const mc_env* e) {
+    return (long long)e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
+}
+
+static void ragged_kps(const mc_ragged* r, std::vector<const mc_kp*>* kps) {
+    kps->clear();
+    for (auto* e : r->envs) kps->push_back(&e->kp);
+}
+
+static void ragged_layout(const mc_ragged* r, const mc_ragged_config* c, mc_ragged_kp* rk) {
+    std::vector<const mc_kp*> kps;
+    ragged_kps(r, &kps);
+    team_layout(kps.data(), (int)kps.size(), c->stage, c->tile_w, c->coop, c->team_warps, c->warps_per_cta, rk);
+    rk->flags = r->flags;
+}
+
+static int ragged_validate(const mc_ragged* r, const mc_ragged_config* c) {
+    std::vector<const mc_kp*> kps;
+    ragged_kps(r, &kps);
+    return team_validate(kps.data(), (int)kps.size(), c->stage, c->tile_w, c->coop, c->team_warps, c->warps_per_cta,
+                         c->ctas_per_sm);
+}
+
+static void ragged_default_config(mc_ragged* r) {
+    // teams of 8 warps; groups with big images or big worlds render each env
+    // as a team, small ones one env per warp; small worlds are staged
+    r->cfg = mc_ragged_config{};
+    r->cfg.warps_per_cta = 8;
+    r->cfg.ctas_per_sm = 4;
+    r->cfg.team_warps = 8;
+    for (size_t g = 0; g < r->envs.size(); ++g) {
+        const mc_env* e = r->envs[g];
+        const long long wxyz = ragged_wxyz(e);
+        const bool big = (long long)e->cfg.render_width * e->cfg.render_height >= 64 * 64 || wxyz > 8192;
+        r->cfg.coop[g] = big ? 1 : 0;
+        r->cfg.stage[g] = (wxyz <= (big ? 32768 : 4096) && (wxyz & 15) == 0 && !(((uintptr_t)e->kp.voxels) & 15));
+        r->cfg.tile_w[g] = big ? 8 : 4;
+    }
+}
+
+static void ragged_drop_graphs(mc_ragged* r) {
+    for (auto& g : r->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    r->graphs.clear();
+}
+
+// The launch copies the groups' parameter blocks by value; when one of them
+// changed (an env handle was re-pointed), cached graphs hold stale copies.
+static int ragged_sync_groups(mc_ragged* r, bool capturing) {
+    bool same = r->uploaded.size() == r->envs.size();
+    for (size_t g = 0; same && g < r->envs.size(); ++g)
+        same = memcmp(&r->uploaded[g], &r->envs[g]->kp, sizeof(mc_kp)) == 0;
+    if (same) return MC_OK;
+    if (capturing) return fail(MC_ERR_INVALID, "a group was re-pointed; step once outside capture first");
+    r->uploaded.clear();
+    for (auto* e : r->envs) r->uploaded.push_back(e->kp);
+    ++r->version;
+    ragged_drop_graphs(r);
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_create(mc_env* const* groups, int32_t ngroups, mc_ragged** out) {
+    if (!out) return fail(MC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!groups || ngroups < 1 || ngroups > MC_RAGGED_MAX_GROUPS)
+        return fail(MC_ERR_INVALID, "ngroups must be 1..%d", MC_RAGGED_MAX_GROUPS);
+    long long total = 0;
+    for (int g = 0; g < ngroups; ++g) {
+        const mc_env* e = groups[g];
+        if (!e) return fail(MC_ERR_INVALID, "group %d is NULL", g);
+        for (int h = 0; h < g; ++h)
+            if (groups[h] == e) return fail(MC_ERR_INVALID, "group %d repeats group %d", g, h);
+        if (e->device != groups[0]->device) return fail(MC_ERR_INVALID, "group %d is on another device", g);
+        if (e->cfg.numerics != groups[0]->cfg.numerics) return fail(MC_ERR_INVALID, "group %d: other numerics", g);
+        if (e->kp.family != groups[0]->kp.family || e->kp.obs_f32 != groups[0]->kp.obs_f32)
+            return fail(MC_ERR_INVALID, "group %d: another observation kind (obs_mode)", g);
+        total += e->cfg.batch_size;
+    }
+    if (total > (1LL << 30)) return fail(MC_ERR_INVALID, "more than 2^30 envs in one ragged handle");
+    int dev = -1;
+    MC_CK(cudaGetDevice(&dev));
+    if (dev != groups[0]->device) return fail(MC_ERR_INVALID, "the groups live on device %d, current is %d",
+                                              groups[0]->device, dev);
+    mc_ragged* r = new mc_ragged();
+    r->envs.assign(groups, groups + ngroups);
+    r->be = groups[0]->be;
+    r->family = groups[0]->kp.family;
+    r->obs_f32 = groups[0]->kp.obs_f32;
+    r->device = dev;
+    r->num_sms = groups[0]->num_sms;
+    cudaError_t ce = cudaMalloc(&r->flags, MC_FLAG_WORDS * sizeof(int32_t));
+    if (ce == cudaSuccess) ce = cudaMemset(r->flags, 0, MC_FLAG_WORDS * sizeof(int32_t));
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        int rc = cuda_fail(ce, "mc_ragged_create");
+        mc_ragged_destroy(r);
+        return rc;
+    }
+    ragged_default_config(r);
+    if (ragged_validate(r, &r->cfg) != MC_OK) {  // e.g. unaligned voxels: no staging
+        for (int g = 0; g < ngroups; ++g) r->cfg.stage[g] = 0;
+    }
+    ragged_sync_groups(r, false);
+    *out = r;
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_destroy(mc_ragged* r) {
+    if (!r) return MC_OK;
+    ragged_drop_graphs(r);
+    if (r->flags) cudaFree(r->flags);
+    if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
+    delete r;
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_set_config(mc_ragged* r, const mc_ragged_config* c) {
+    if (!r || !c) return fail(MC_ERR_INVALID, "NULL argument");
+    int rc = ragged_validate(r, c);
+    if (rc) return rc;
+    r->cfg = *c;
+    for (size_t g = r->envs.size(); g < MC_RAGGED_MAX_GROUPS; ++g) r->cfg.stage[g] = r->cfg.tile_w[g] = r->cfg.coop[g] = 0;
+    ++r->version;
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_get_config(const mc_ragged* r, mc_ragged_config* c) {
+    if (!r || !c) return fail(MC_ERR_INVALID, "NULL argument");
+    *c = r->cfg;
+    return MC_OK;
+}
+
+extern "C" int64_t mc_ragged_total_envs(const mc_ragged* r) {
+    if (!r) return -1;
+    long long t = 0;
+    for (auto* e : r->envs) t += e->cfg.batch_size;
+    return t;
+}
+
+extern "C" int64_t mc_ragged_smem_bytes(const mc_ragged* r) {
+    if (!r) return -1;
+    mc_ragged_kp rk;
+    ragged_layout(r, &r->cfg, &rk);
+    return team_smem(rk, r->cfg.warps_per_cta);
+}
+
+static int ragged_do_step(mc_ragged* r, const int8_t* buttons, const float* look, const uint8_t* actions,
+                          cudaStream_t s, bool capturing) {
+    int rc = ragged_sync_groups(r, capturing);
+    if (rc) return rc;
+    mc_ragged_kp rk;
+    ragged_layout(r, &r->cfg, &rk);
+    rk.actions = actions;
+    rk.buttons = buttons;
+    rk.look = look;
+    rc = backend_rc(r->be->step_team(&rk, r->family, r->obs_f32, r->cfg.warps_per_cta, r->cfg.ctas_per_sm,
+                                     r->num_sms, s),
+                    "step_team");
+    if (rc) return rc;
+    for (auto* e : r->envs)
+        if (e->cfg.batch_size > 0 && dones_possible(e->kp)) {
+            rc = backend_rc(mc_launch_regen(&e->kp, 1, s), "regen");
+            if (rc) return rc;
+        }
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* look, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    if (mc_ragged_total_envs(r) > 0 && (!buttons || !look)) return fail(MC_ERR_INVALID, "buttons/look are NULL");
+    if (((uintptr_t)look) & 3) return fail(MC_ERR_INVALID, "look must be 4-byte aligned");
+    return ragged_do_step(r, buttons, look, nullptr, (cudaStream_t)stream, false);
+}
+
+extern "C" int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    if (mc_ragged_total_envs(r) > 0 && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    return ragged_do_step(r, nullptr, nullptr, actions, (cudaStream_t)stream, false);
+}
+
+static int ragged_graph(mc_ragged* r, const uint8_t* actions, int32_t K, RaggedGraph** out) {
+    *out = nullptr;
+    int rc = ragged_sync_groups(r, false);
+    if (rc) return rc;
+    for (auto& g : r->graphs)
+        if (g.actions == actions && g.K == K && g.version == r->version) {
+            *out = &g;
+            return MC_OK;
+        }
+    const long long total = mc_ragged_total_envs(r);
+    cudaGraph_t graph = nullptr;
+    MC_CK(cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < K && rc == MC_OK; ++k)
+        rc = ragged_do_step(r, nullptr, nullptr, actions + (long long)k * total, r->cap_stream, true);
+    cudaError_t ce = cudaStreamEndCapture(r->cap_stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    RaggedGraph g;
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    g.actions = actions;
+    g.K = K;
+    g.version = r->version;
+    if (r->graphs.size() >= 8) {
+        cudaGraphExecDestroy(r->graphs.front().exec);
+        r->graphs.erase(r->graphs.begin());
+    }
+    r->graphs.push_back(g);
+    *out = &r->graphs.back();
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_rollout_prepare(mc_ragged* r, const uint8_t* actions, int32_t K) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    if (K < 0) return fail(MC_ERR_INVALID, "K < 0");
+    if (K == 0 || mc_ragged_total_envs(r) == 0) return MC_OK;
+    if (!actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    RaggedGraph* g;
+    return ragged_graph(r, actions, K, &g);
+}
+
+extern "C" int mc_ragged_rollout(mc_ragged* r, const uint8_t* actions, int32_t K, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    if (K < 0) return fail(MC_ERR_INVALID, "K < 0");
+    if (K == 0 || mc_ragged_total_envs(r) == 0) return MC_OK;
+    if (!actions) return fail(MC_ERR_INVALID, "actions is NULL");
+    RaggedGraph* g;
+    int rc = ragged_graph(r, actions, K, &g);
+    if (rc) return rc;
+    MC_CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return MC_OK;
+}
+
+extern "C" int mc_ragged_check_error(mc_ragged* r, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    for (auto* e : r->envs) {
+        int rc = mc_env_check_error(e, stream);
+        if (rc) return rc;
     }
     return MC_OK;
 }
@@ -892,7 +1284,9 @@ extern "C" int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* s
         f.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
         f.warps_per_cta = 8;
         f.ctas_per_sm = 4;
-        f.tile_w = 8;
+        f.tile_w = 4;
+        f.team_warps = 1;
+        f.coop = 0;
         return backend_rc(be->step_fused(&k, &f, sms, (cudaStream_t)stream), "step_fused");
     }
     return fail(MC_ERR_INVALID, "unknown form %d", form);

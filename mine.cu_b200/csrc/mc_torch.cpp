@@ -8,6 +8,8 @@
 // properties, src/bindings.cpp:223-228, 453-457), and calls the C-ABI of
 // libminecu_b200.so on torch's current CUDA stream.
 #include <torch/extension.h>
+
+#include <vector>
 #include <ATen/cuda/CUDAContext.h>
 #include <c10/cuda/CUDAGuard.h>
 
@@ -490,8 +492,9 @@ void env_rollout_prepare(std::shared_ptr<Env> e, torch::Tensor actions, c10::opt
        "rollout_prepare");
 }
 
-void env_set_fused(std::shared_ptr<Env> e, int stage, int warps_per_cta, int ctas_per_sm, int tile_w) {
-    mc_fused_config f{stage, warps_per_cta, ctas_per_sm, tile_w};
+void env_set_fused(std::shared_ptr<Env> e, int stage, int warps_per_cta, int ctas_per_sm, int tile_w, int team_warps,
+                   int coop) {
+    mc_fused_config f{stage, warps_per_cta, ctas_per_sm, tile_w, team_warps, coop};
     ck(mc_env_set_fused_config(e->h, &f), "set_fused_config");
 }
 
@@ -503,11 +506,98 @@ py::dict env_get_fused(std::shared_ptr<Env> e) {
     d["warps_per_cta"] = f.warps_per_cta;
     d["ctas_per_sm"] = f.ctas_per_sm;
     d["tile_w"] = f.tile_w;
+    d["team_warps"] = f.team_warps;
+    d["coop"] = f.coop;
     d["smem_bytes"] = mc_env_fused_smem_bytes(e->h);
     return d;
 }
 
 void env_check_error(std::shared_ptr<Env> e) { ck(mc_env_check_error(e->h, cur_stream()), "check_error"); }
+
+// ragged handle: several Env handles stepped by one launch
+struct Ragged {
+    mc_ragged* h = nullptr;
+    std::vector<std::shared_ptr<Env>> groups;  // keeps the borrowed env handles alive
+    ~Ragged() {
+        if (h) mc_ragged_destroy(h);
+    }
+};
+
+std::shared_ptr<Ragged> ragged_create(std::vector<std::shared_ptr<Env>> groups) {
+    auto r = std::make_shared<Ragged>();
+    std::vector<mc_env*> hs;
+    for (auto& g : groups) {
+        TORCH_CHECK(g && g->h, "ragged_create: a group is not a live env handle");
+        hs.push_back(g->h);
+    }
+    r->groups = groups;
+    ck(mc_ragged_create(hs.data(), (int32_t)hs.size(), &r->h), "ragged_create");
+    return r;
+}
+
+void ragged_set_config(std::shared_ptr<Ragged> r, int warps_per_cta, int ctas_per_sm, int team_warps,
+                       std::vector<int> stage, std::vector<int> tile_w, std::vector<int> coop) {
+    const size_t G = r->groups.size();
+    TORCH_CHECK(stage.size() == G && tile_w.size() == G && coop.size() == G,
+                "one stage, one tile_w and one coop per group");
+    mc_ragged_config c{};
+    c.warps_per_cta = warps_per_cta;
+    c.ctas_per_sm = ctas_per_sm;
+    c.team_warps = team_warps;
+    for (size_t g = 0; g < G; ++g) {
+        c.stage[g] = stage[g];
+        c.tile_w[g] = tile_w[g];
+        c.coop[g] = coop[g];
+    }
+    ck(mc_ragged_set_config(r->h, &c), "ragged_set_config");
+}
+
+py::dict ragged_get_config(std::shared_ptr<Ragged> r) {
+    mc_ragged_config c{};
+    ck(mc_ragged_get_config(r->h, &c), "ragged_get_config");
+    std::vector<int> st, tw, co;
+    for (size_t g = 0; g < r->groups.size(); ++g) {
+        st.push_back(c.stage[g]);
+        tw.push_back(c.tile_w[g]);
+        co.push_back(c.coop[g]);
+    }
+    py::dict d;
+    d["warps_per_cta"] = c.warps_per_cta;
+    d["ctas_per_sm"] = c.ctas_per_sm;
+    d["team_warps"] = c.team_warps;
+    d["stage"] = st;
+    d["tile_w"] = tw;
+    d["coop"] = co;
+    d["smem_bytes"] = mc_ragged_smem_bytes(r->h);
+    return d;
+}
+
+int64_t ragged_total_envs(std::shared_ptr<Ragged> r) { return mc_ragged_total_envs(r->h); }
+
+void ragged_step(std::shared_ptr<Ragged> r, torch::Tensor buttons, torch::Tensor look) {
+    need(buttons, "buttons", at::kChar);
+    need(look, "look", at::kFloat);
+    const int64_t n = mc_ragged_total_envs(r->h);
+    TORCH_CHECK(buttons.numel() == n * 8 && look.numel() == n * 2, "buttons [total,8], look [total,2]");
+    ck(mc_ragged_step(r->h, ptr<int8_t>(buttons), ptr<float>(look), cur_stream()), "ragged_step");
+}
+
+void ragged_step_discrete(std::shared_ptr<Ragged> r, torch::Tensor actions) {
+    need(actions, "actions", at::kByte);
+    TORCH_CHECK(actions.numel() == mc_ragged_total_envs(r->h), "actions must hold one action per env");
+    ck(mc_ragged_step_discrete(r->h, ptr<uint8_t>(actions), cur_stream()), "ragged_step");
+}
+
+void ragged_rollout(std::shared_ptr<Ragged> r, torch::Tensor actions, bool prepare_only) {
+    need(actions, "actions", at::kByte);
+    TORCH_CHECK(actions.dim() == 2 && actions.size(1) == mc_ragged_total_envs(r->h), "actions must be [K, total]");
+    if (prepare_only)
+        ck(mc_ragged_rollout_prepare(r->h, ptr<uint8_t>(actions), (int32_t)actions.size(0)), "ragged_rollout_prepare");
+    else
+        ck(mc_ragged_rollout(r->h, ptr<uint8_t>(actions), (int32_t)actions.size(0), cur_stream()), "ragged_rollout");
+}
+
+void ragged_check_error(std::shared_ptr<Ragged> r) { ck(mc_ragged_check_error(r->h, cur_stream()), "check_error"); }
 
 void philox_actions(torch::Tensor out, int env_offset, int step0, uint64_t seed, bool break_half) {
     need(out, "out", at::kByte);
@@ -597,6 +687,15 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("env_set_fused", &env_set_fused);
     m.def("env_get_fused", &env_get_fused);
     m.def("env_check_error", &env_check_error);
+    py::class_<Ragged, std::shared_ptr<Ragged>>(m, "Ragged");
+    m.def("ragged_create", &ragged_create);
+    m.def("ragged_set_config", &ragged_set_config);
+    m.def("ragged_get_config", &ragged_get_config);
+    m.def("ragged_total_envs", &ragged_total_envs);
+    m.def("ragged_step", &ragged_step);
+    m.def("ragged_step_discrete", &ragged_step_discrete);
+    m.def("ragged_rollout", &ragged_rollout, py::arg("ragged"), py::arg("actions"), py::arg("prepare_only") = false);
+    m.def("ragged_check_error", &ragged_check_error);
     m.def("philox_actions", &philox_actions, py::arg("out"), py::arg("env_offset"), py::arg("step0"),
           py::arg("seed"), py::arg("break_half") = false);
     m.def("discrete_to_buttons", &discrete_to_buttons);

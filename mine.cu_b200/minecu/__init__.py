@@ -344,9 +344,13 @@ class MineEnv:
         return (self.render_height, self.render_width, 3)
 
     # ------------------------------------------------------------------
-    def set_launch_config(self, stage: int, warps_per_cta: int, ctas_per_sm: int, tile_w: int) -> None:
-        """Launch shape of the fused kernel (see minecu.autotune)."""
-        _C.env_set_fused(self._env, int(stage), int(warps_per_cta), int(ctas_per_sm), int(tile_w))
+    def set_launch_config(self, stage: int, warps_per_cta: int, ctas_per_sm: int, tile_w: int,
+                          team_warps: int = 1, coop: int = 0) -> None:
+        """Launch shape of the fused step (see minecu.autotune).  team_warps=1,
+        coop=0: one warp steps and renders each env; coop=1: a team of
+        team_warps warps renders each env together."""
+        _C.env_set_fused(self._env, int(stage), int(warps_per_cta), int(ctas_per_sm), int(tile_w), int(team_warps),
+                         int(coop))
 
     def launch_config(self) -> dict:
         return _C.env_get_fused(self._env)

@@ -48,13 +48,22 @@ class EnvState(ctypes.Structure):
 
 class FusedConfig(ctypes.Structure):
     _fields_ = [("stage", c_int32), ("warps_per_cta", c_int32), ("ctas_per_sm", c_int32),
-                ("tile_w", c_int32)]
+                ("tile_w", c_int32), ("team_warps", c_int32), ("coop", c_int32)]
 
 
 class DecodeBuffers(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in (
         "forward_in", "strafe_in", "delta_yaw_in", "delta_pitch_in", "jump_in", "do_break", "do_place",
         "speed_mult")]
+
+
+RAGGED_MAX_GROUPS = 16
+
+
+class RaggedConfig(ctypes.Structure):
+    _fields_ = [("warps_per_cta", c_int32), ("ctas_per_sm", c_int32), ("team_warps", c_int32),
+                ("stage", c_int32 * RAGGED_MAX_GROUPS), ("tile_w", c_int32 * RAGGED_MAX_GROUPS),
+                ("coop", c_int32 * RAGGED_MAX_GROUPS)]
 
 
 P, I, F, U32, U64 = c_void_p, c_int32, c_float, ctypes.c_uint32, ctypes.c_uint64
@@ -77,6 +86,17 @@ _PROTOS = {
     "mc_env_get_fused_config": (I, [P, ctypes.POINTER(FusedConfig)]),
     "mc_env_check_error": (I, [P, P]),
     "mc_env_fused_smem_bytes": (ctypes.c_int64, [P]),
+    "mc_ragged_create": (I, [ctypes.POINTER(c_void_p), I, ctypes.POINTER(c_void_p)]),
+    "mc_ragged_destroy": (I, [P]),
+    "mc_ragged_set_config": (I, [P, ctypes.POINTER(RaggedConfig)]),
+    "mc_ragged_get_config": (I, [P, ctypes.POINTER(RaggedConfig)]),
+    "mc_ragged_total_envs": (ctypes.c_int64, [P]),
+    "mc_ragged_smem_bytes": (ctypes.c_int64, [P]),
+    "mc_ragged_step": (I, [P, P, P, P]),
+    "mc_ragged_step_discrete": (I, [P, P, P]),
+    "mc_ragged_rollout": (I, [P, P, I, P]),
+    "mc_ragged_rollout_prepare": (I, [P, P, I]),
+    "mc_ragged_check_error": (I, [P, P]),
     "mc_generate_world": (I, [P, I, I, I, I, I, U32, P]),
     "mc_place_tree": (I, [P, I, I, I, I, I, I, I, P]),
     "mc_place_house": (I, [P, I, I, I, I, I, I, I, P]),

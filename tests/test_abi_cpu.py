@@ -13,7 +13,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 25
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.mc_abi_version() == 1
+    assert L.mc_abi_version() == 2
 
 
 def test_prototypes_cover_header():
@@ -65,3 +65,19 @@ def test_stateless_entry_points_validate_before_launch():
     # zero-sized work is a no-op, not an error
     assert L.mc_generate_world(None, 0, 8, 8, 8, 4, 0, None) == capi.MC_OK
     assert L.mc_env_destroy(None) == capi.MC_OK
+
+
+def test_ragged_entry_points_validate_before_launch():
+    L = capi.lib()
+    out = ctypes.c_void_p()
+    assert L.mc_ragged_create(None, 2, ctypes.byref(out)) == capi.MC_ERR_INVALID
+    groups = (ctypes.c_void_p * 17)()
+    assert L.mc_ragged_create(groups, 17, ctypes.byref(out)) == capi.MC_ERR_INVALID
+    assert "ngroups" in capi.last_error()
+    assert L.mc_ragged_create(groups, 2, ctypes.byref(out)) == capi.MC_ERR_INVALID  # NULL groups
+    assert not out.value
+    assert L.mc_ragged_step_discrete(None, None, None) == capi.MC_ERR_INVALID
+    assert L.mc_ragged_rollout(None, None, 4, None) == capi.MC_ERR_INVALID
+    assert L.mc_ragged_set_config(None, None) == capi.MC_ERR_INVALID
+    assert L.mc_ragged_total_envs(None) == -1
+    assert L.mc_ragged_destroy(None) == capi.MC_OK

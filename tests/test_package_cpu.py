@@ -10,7 +10,7 @@ from minecu.config import FAST_ENV, QUALITY_ENV
 def test_extension_is_the_in_tree_build():
     import os
     assert os.path.dirname(minecu._C.__file__) == os.path.dirname(minecu.__file__)
-    assert minecu._C.ABI_VERSION == 1
+    assert minecu._C.ABI_VERSION == 2
     for name in ("render", "render_uint8", "physics", "raycast_break", "reset", "generate_world", "place_tree",
                  "place_house", "step", "step_uint8", "step_uint8_fast", "step_uint8_minimal", "step_uint8_fp16",
                  "step_uint8_prebasis", "step_uint8_prebasis_full", "step_uint8_smem", "precompute_camera_basis",
