@@ -541,6 +541,105 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# Serving: 16 client jobs, batch log-uniform in [256, 8192], world 16^3 or
+# 32^3, 32x32 or 64x64 uint8 observations, episodes of 200..2000 steps (a
+# reset request between episodes), Poisson arrivals at the same request rate
+# for every job (offered env-steps/s = rate x total envs), HBM budget 150 GB.
+# The server queues up to 2 launches on the device and caps one launch at
+# 16,384 envs.
+SERVE_SEED = 5
+SERVE_LOADS = (0.2, 0.4, 0.6, 0.8, 1.0, 1.2)
+SERVE_METRIC = "served env-steps/s at p99 step latency < 2 ms (16 jobs, mixed sizes, Poisson arrivals)"
+
+
+def serve_jobs(n=16, seed=SERVE_SEED):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(n):
+        b = int(round(float(np.exp(rng.uniform(np.log(256), np.log(8192))))))
+        jobs.append(dict(batch=b, world=int(rng.choice([16, 32])), res=int(rng.choice([32, 64])),
+                         episode=int(rng.integers(200, 2001))))
+    return jobs
+
+
+def run_mine_serve(args):
+    import torch
+    from minecu.server import EnvServer
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    jobs = serve_jobs()
+    secs = args.serve_seconds
+
+    def make(batching):
+        srv = EnvServer(hbm_budget_bytes=150e9, batching=batching, max_inflight=2, max_envs_per_launch=16384,
+                        device=dev)
+        ids = [srv.admit(j["batch"], world_size=j["world"], render_width=j["res"], render_height=j["res"])
+               for j in jobs]
+        return srv, ids
+
+    def sweep(srv, ids, peak):
+        out = []
+        total = sum(j["batch"] for j in jobs)
+        for frac in SERVE_LOADS:
+            rates = [frac * peak / total for _ in jobs]
+            st = srv.drive([(i, r, j["episode"], k + 1) for k, (i, r, j) in enumerate(zip(ids, rates, jobs))],
+                           seconds=secs)
+            out.append({"offered_frac": frac, "offered_env_steps_per_s": frac * peak,
+                        "env_steps_per_s": st["env_steps_per_s"], "p50_us": st["p50_us"], "p99_us": st["p99_us"],
+                        "max_us": st["max_us"], "step_requests": st["step_requests"],
+                        "reset_requests": st["reset_requests"], "mean_jobs_per_launch": st["mean_jobs_per_launch"]})
+        return out
+
+    results = {}
+    with ClockSampler(local) as clk:
+        for name, batching in (("batched", True), ("plain", False)):
+            srv, ids = make(batching)
+            srv.drive([(i, 0.0, 0, k + 1) for k, i in enumerate(ids)], seconds=0.5, closed_loop=True)  # warm-up
+            peak = srv.drive([(i, 0.0, j["episode"], k + 1) for k, (i, j) in enumerate(zip(ids, jobs))],
+                             seconds=secs, closed_loop=True)
+            results[name] = {"closed_loop_env_steps_per_s": peak["env_steps_per_s"],
+                             "closed_loop_p50_us": peak["p50_us"], "closed_loop_p99_us": peak["p99_us"]}
+            if name == "batched":
+                ref_peak = peak["env_steps_per_s"]
+            results[name]["sweep"] = sweep(srv, ids, ref_peak)
+            srv.close()
+    ok = [r for r in results["batched"]["sweep"] if r["p99_us"] < 2000.0]
+    value = max((r["env_steps_per_s"] for r in ok), default=0.0)
+    plain_ok = [r for r in results["plain"]["sweep"] if r["p99_us"] < 2000.0]
+    peak, peak_kind = load_peaks()
+    mean_bytes = sum(j["batch"] * (j["world"] ** 3 + j["res"] ** 2 * 3) for j in jobs) / sum(j["batch"] for j in jobs)
+    achieved = value * mean_bytes / 1e9
+    line = {
+        "metric": SERVE_METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": None,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
+        "config": {"workload": "serving: 16 jobs " + ", ".join(f"({j['batch']}, {j['world']}^3, {j['res']}^2, "
+                                                               f"ep {j['episode']})" for j in jobs),
+                   "hbm_budget_bytes": 150e9, "arrivals": "Poisson per job, the same request rate for every job",
+                   "server": {"max_inflight": 2, "max_envs_per_launch": 16384},
+                   "offered_loads": list(SERVE_LOADS), "seconds_per_level": secs, "numerics": "ref_fast",
+                   "latency": "request submission to rewards/dones in host memory"},
+        "batched": results["batched"], "plain_one_job_at_a_time": results["plain"],
+        "sustained_vs_closed_loop_peak": value / results["batched"]["closed_loop_env_steps_per_s"]
+        if results["batched"]["closed_loop_env_steps_per_s"] else None,
+        "plain_value": max((r["env_steps_per_s"] for r in plain_ok), default=0.0),
+        "e2e": {"value": value, "unit": "env-steps/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "path": "EnvServer requests: host actions in, host rewards+dones out (every request)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_env_step": mean_bytes,
+                     "kernel": "k_step_team (served launches)"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def run_reference_ragged(args):
     """The ragged workload on the reference's own CUDA build: the reference
     runs one world size and resolution per MineEnv, so the 6 groups are 6
@@ -636,15 +735,23 @@ def main():
     ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,tile_w")
     ap.add_argument("--traffic-bytes", type=float, default=0.0,
                     help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--workload", default="peak", choices=["peak", "ragged"],
-                    help="peak: B=32768, 16^3, 32x32 (default); ragged: 24,576 envs in 6 groups")
+    ap.add_argument("--workload", default="peak", choices=["peak", "ragged", "serve"],
+                    help="peak: B=32768, 16^3, 32x32 (default); ragged: 24,576 envs in 6 groups; "
+                         "serve: the env server under Poisson load")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds per offered-load level (serve)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
-        run_reference_ragged(args) if args.workload == "ragged" else run_reference(args)
+        if args.workload == "serve":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no env server; the "
+                              "one-job-at-a-time loop is the serve line's plain_one_job_at_a_time arm"}))
+        elif args.workload == "ragged":
+            run_reference_ragged(args)
+        else:
+            run_reference(args)
     else:
-        run_mine_ragged(args) if args.workload == "ragged" else run_mine(args)
+        {"peak": run_mine, "ragged": run_mine_ragged, "serve": run_mine_serve}[args.workload](args)
 
 
 if __name__ == "__main__":

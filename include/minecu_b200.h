@@ -38,6 +38,9 @@ extern "C" {
 #define MC_ERR_CUDA (-2)        /* a CUDA runtime call failed */
 #define MC_ERR_KERNEL (-3)      /* a kernel recorded an error (bounded wait expired) */
 #define MC_ERR_UNSUPPORTED (-4) /* configuration not supported by this build */
+#define MC_ERR_BUDGET (-5)      /* env server: admission would exceed the HBM budget */
+#define MC_ERR_TIMEOUT (-6)     /* env server: the wait ended before the request completed */
+#define MC_ERR_BUSY (-7)        /* env server: the job still has requests queued or running */
 
 /* numerics modes */
 #define MC_NUMERICS_REF_FAST 0 /* same fast-math CUDA calls and op order as the reference build */
@@ -196,6 +199,85 @@ int mc_ragged_rollout(mc_ragged* r, const uint8_t* actions, int32_t K, void* str
 int mc_ragged_rollout_prepare(mc_ragged* r, const uint8_t* actions, int32_t K);
 /* Reads and clears the device error words of the launch and of every group. */
 int mc_ragged_check_error(mc_ragged* r, void* stream);
+
+/* ---- env server: many client jobs on one device ----------------------
+ * No counterpart in the reference (one Python MineEnv per process, stepped
+ * by its owner).  A server owns the device state of many jobs (each job is
+ * one env configuration: batch, world, resolution, ...), admitted against
+ * an HBM budget, and serves step/reset requests from client threads.  A
+ * launcher thread takes the oldest queued request of every job with work
+ * and runs them together: resets as MineEnv.reset, steps as one launch of
+ * the team kernel over the jobs (groups of up to MC_RAGGED_MAX_GROUPS), with
+ * one actions upload and one rewards/dones read-back per launch.  A job's
+ * requests run in submission order; each step's results equal
+ * mc_env_step_discrete with the fused form on that job alone.  With
+ * batching = 0 the server runs one request at a time, in arrival order, with
+ * the plain form (the one-job-at-a-time loop the batching is compared to).
+ * Latency = request submission to results in host memory. */
+#define MC_REQ_STEP 0
+#define MC_REQ_RESET 1
+typedef struct mc_server mc_server;
+typedef struct mc_server_config {
+    int64_t hbm_budget_bytes;   /* admission budget for the jobs' device state (mc_server_job_bytes) */
+    int32_t numerics;           /* MC_NUMERICS_*, shared by every job */
+    int32_t batching;           /* 1: batch one request per job into team launches; 0: one request at a time */
+    int32_t max_inflight;       /* launches queued on the device at once, 1..4 */
+    int32_t max_envs_per_launch;/* cap on the envs of one step launch (0: 1 << 20) */
+} mc_server_config;
+typedef struct mc_server_stats {
+    int64_t step_requests;      /* completed since create / mc_server_reset_stats */
+    int64_t reset_requests;
+    int64_t env_steps;
+    int64_t launches;           /* step launches */
+    double elapsed_s;           /* since create / reset */
+    double env_steps_per_s;     /* env_steps / elapsed_s */
+    double p50_us, p90_us, p99_us, max_us, mean_us; /* step latency */
+    double reset_p50_us, reset_p99_us;
+    double mean_jobs_per_launch;
+    int32_t jobs;               /* admitted now */
+    int64_t bytes_admitted;
+} mc_server_stats;
+int mc_server_create(const mc_server_config* cfg, mc_server** out);
+/* Stops the threads after the requests already queued have run. */
+int mc_server_destroy(mc_server* s);
+/* Device bytes one job of this configuration is charged at admission. */
+int64_t mc_server_job_bytes(const mc_env_config* cfg);
+/* Allocate and generate a job's worlds and spawn its agents (as MineEnv(...)
+ * followed by reset()); MC_ERR_BUDGET if it does not fit. */
+int mc_server_admit(mc_server* s, const mc_env_config* cfg, int32_t* job);
+/* Free a job; MC_ERR_BUSY while it has requests queued or running. */
+int mc_server_release(mc_server* s, int32_t job);
+/* The job's device state (observations, rewards, ... as MineEnv tensors). */
+int mc_server_job_state(mc_server* s, int32_t job, mc_env_state* out);
+/* Queue a request: MC_REQ_STEP with host actions uint8[batch] (copied), or
+ * MC_REQ_RESET (actions unused).  The ticket is passed to mc_server_wait. */
+int mc_server_submit(mc_server* s, int32_t job, int32_t kind, const uint8_t* actions, int64_t* ticket);
+/* Wait for a request; rewards float[batch] and dones uint8[batch] (host,
+ * optional) receive a step's results.  timeout_us < 0 waits for ever;
+ * MC_ERR_TIMEOUT leaves the ticket valid. */
+int mc_server_wait(mc_server* s, int64_t ticket, float* rewards, uint8_t* dones, int64_t timeout_us);
+int mc_server_get_stats(mc_server* s, mc_server_stats* out);
+int mc_server_reset_stats(mc_server* s);
+/* Load generator: one client thread per entry, each issuing requests for
+ * its job for `seconds` - open loop with Poisson arrivals at rate_hz, or
+ * closed loop (the next request when the last one completed) - with a reset
+ * every episode_steps steps and uniform discrete actions from Philox
+ * (seed, job env, step).  Waits for every issued request, then fills `out`
+ * with the latencies of the requests issued in the window and the env-steps
+ * completed in it. */
+typedef struct mc_load_job {
+    int32_t job;
+    double rate_hz;             /* open loop: mean requests per second */
+    int32_t episode_steps;      /* steps between reset requests (0: none) */
+    uint32_t seed;
+} mc_load_job;
+typedef struct mc_load_config {
+    double seconds;
+    int32_t closed_loop;
+    int32_t njobs;
+    const mc_load_job* jobs;
+} mc_load_config;
+int mc_server_drive(mc_server* s, const mc_load_config* cfg, mc_server_stats* out);
 
 /* ---- stateless kernels: the reference's _C functions ------------------ */
 /* generate_world_kernel (src/kernels.cu:1793-1828) via launch_generate_world

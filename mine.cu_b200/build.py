@@ -35,6 +35,7 @@ UNITS = {
     "mc_ieee": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "mc_runtime": [],
     "mc_noalloc": [],
+    "mc_server": [],
 }
 
 

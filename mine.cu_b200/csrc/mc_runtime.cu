@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/minecu_b200.h"
+#include "mc_env_impl.h"
 #include "mc_internal.h"
 #include "mc_philox.h"
 
@@ -51,6 +52,16 @@ static int backend_rc(int rc, const char* what) {
 }
 
 int mc_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int mc_fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int mc_cuda_fail(cudaError_t e, const char* what) { return cuda_fail(e, what); }
 
 extern "C" int mc_abi_version(void) { return MC_ABI_VERSION; }
 extern "C" const char* mc_last_error(void) { return g_err; }
@@ -378,32 +389,7 @@ static int check_state(const mc_env_config* c, const mc_env_state* s) {
 // ---------------------------------------------------------------------------
 // env handle
 // ---------------------------------------------------------------------------
-struct RolloutGraph {
-    cudaGraphExec_t exec = nullptr;
-    const uint8_t* actions = nullptr;
-    float* rewards_out = nullptr;
-    uint8_t* dones_out = nullptr;
-    int K = 0;
-    mc_fused_cfg fcfg{};
-    mc_kp kp{};
-};
-
-struct mc_env {
-    mc_env_config cfg;
-    mc_env_state st;
-    mc_kp kp;
-    const mc_backend* be;
-    int device;
-    int num_sms;
-    mc_fused_cfg fcfg;
-    int32_t* flags;
-    int8_t* tmpl;
-    uint8_t* scratch;  // plain-form decode buffers
-    cudaStream_t cap_stream;
-    std::vector<RolloutGraph> graphs;
-};
-
-static bool dones_possible(const mc_kp& k) {
+bool dones_possible(const mc_kp& k) {
     if (k.ext_done) return false;
     if (k.episode_rule == 0) return k.has_limit != 0;
     return k.episode_length > 0;
@@ -411,10 +397,7 @@ static bool dones_possible(const mc_kp& k) {
 
 static inline int align16i(long long x) { return (int)((x + 15) & ~15LL); }
 
-// Launch description of the team kernel over G groups (host copies of their
-// parameter blocks, copied into the launch's parameter block); flags and
-// actions are left to the caller.
-static void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
+void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
                         int team_warps, int warps_per_cta, mc_ragged_kp* rk) {
     *rk = mc_ragged_kp{};
     rk->ngroups = G;
@@ -466,11 +449,11 @@ static void team_layout(const mc_kp* const* kps, int G, const int* stage, const 
     rk->warp_bytes = 16 + band;
 }
 
-static long long team_smem(const mc_ragged_kp& rk, int warps_per_cta) {
+long long team_smem(const mc_ragged_kp& rk, int warps_per_cta) {
     return (long long)rk.warps_off + (long long)warps_per_cta * rk.warp_bytes;
 }
 
-static int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
+int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
                          int team_warps, int warps_per_cta, int ctas_per_sm) {
     if (warps_per_cta < 1 || warps_per_cta > 8) return fail(MC_ERR_INVALID, "warps_per_cta must be 1..8");
     if (team_warps != 1 && team_warps != 2 && team_warps != 4 && team_warps != 8)
@@ -500,18 +483,6 @@ static int team_validate(const mc_kp* const* kps, int G, const int* stage, const
 
 static bool team_mode(const mc_fused_cfg& f) { return f.team_warps > 1 || f.coop; }
 
-static void default_fused(mc_env* e) {
-    // Staging a world in shared memory pays when it is small; the autotuner
-    // (minecu/autotune.py) refines this per configuration.
-    int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
-    e->fcfg.stage = (wxyz <= 8192 && (wxyz & 15) == 0) ? 1 : 0;
-    e->fcfg.warps_per_cta = 8;
-    e->fcfg.ctas_per_sm = 4;
-    e->fcfg.tile_w = 4;
-    e->fcfg.team_warps = 1;
-    e->fcfg.coop = 0;
-}
-
 static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
     if (team_mode(*f)) {
         const mc_kp* kps[1] = {&e->kp};
@@ -530,6 +501,33 @@ static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
     size_t smem = e->be->fused_smem_bytes(&k, f);
     if (smem > 227 * 1024) return fail(MC_ERR_INVALID, "fused shared memory %zu > 227 KB", smem);
     return MC_OK;
+}
+
+static void default_fused(mc_env* e) {
+    // Small images over small worlds: one warp per env, world staged in
+    // shared memory.  Big images or big worlds: teams of 4 warps render each
+    // env together from one staged copy of its world.  The autotuner
+    // (minecu/autotune.py) refines this per configuration.
+    const int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
+    const bool aligned = (wxyz & 15) == 0 && !(((uintptr_t)e->kp.voxels) & 15);
+    const bool big = e->cfg.render_width * e->cfg.render_height >= 64 * 64 || wxyz > 8192;
+    e->fcfg.warps_per_cta = 8;
+    if (big) {
+        e->fcfg.stage = (wxyz <= 32768 && aligned) ? 1 : 0;
+        e->fcfg.ctas_per_sm = 3;
+        e->fcfg.tile_w = 8;
+        e->fcfg.team_warps = 4;
+        e->fcfg.coop = 1;
+    } else {
+        e->fcfg.stage = (wxyz <= 8192 && aligned) ? 1 : 0;
+        e->fcfg.ctas_per_sm = 4;
+        e->fcfg.tile_w = 4;
+        e->fcfg.team_warps = 1;
+        e->fcfg.coop = 0;
+    }
+    if (validate_fused(e, &e->fcfg) != MC_OK) {  // e.g. a world too big for one team's shared memory
+        e->fcfg.stage = 0;
+    }
 }
 
 static void drop_graphs(mc_env* e) {
@@ -901,7 +899,7 @@ static void ragged_default_config(mc_ragged* r) {
     r->cfg = mc_ragged_config{};
     r->cfg.warps_per_cta = 8;
     r->cfg.ctas_per_sm = 4;
-    r->cfg.team_warps = 8;
+    r->cfg.team_warps = 4;
     for (size_t g = 0; g < r->envs.size(); ++g) {
         const mc_env* e = r->envs[g];
         const long long wxyz = ragged_wxyz(e);

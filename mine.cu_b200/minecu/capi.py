@@ -18,6 +18,8 @@ LIB_PATH = os.path.join(_HERE, "libminecu_b200.so")
 HEADER = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "minecu_b200.h")
 
 MC_OK, MC_ERR_INVALID, MC_ERR_CUDA, MC_ERR_KERNEL, MC_ERR_UNSUPPORTED = 0, -1, -2, -3, -4
+MC_ERR_BUDGET, MC_ERR_TIMEOUT, MC_ERR_BUSY = -5, -6, -7
+REQ_STEP, REQ_RESET = 0, 1
 NOALLOC_MAX_ENVS = 65536
 NUMERICS_REF_FAST, NUMERICS_IEEE = 0, 1
 FORM_PLAIN, FORM_FUSED = 0, 1
@@ -66,6 +68,33 @@ class RaggedConfig(ctypes.Structure):
                 ("coop", c_int32 * RAGGED_MAX_GROUPS)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("numerics", c_int32), ("batching", c_int32),
+                ("max_inflight", c_int32), ("max_envs_per_launch", c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("step_requests", ctypes.c_int64), ("reset_requests", ctypes.c_int64),
+                ("env_steps", ctypes.c_int64), ("launches", ctypes.c_int64), ("elapsed_s", ctypes.c_double),
+                ("env_steps_per_s", ctypes.c_double), ("p50_us", ctypes.c_double), ("p90_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double),
+                ("reset_p50_us", ctypes.c_double), ("reset_p99_us", ctypes.c_double),
+                ("mean_jobs_per_launch", ctypes.c_double), ("jobs", c_int32), ("bytes_admitted", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LoadJob(ctypes.Structure):
+    _fields_ = [("job", c_int32), ("rate_hz", ctypes.c_double), ("episode_steps", c_int32),
+                ("seed", ctypes.c_uint32)]
+
+
+class LoadConfig(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("closed_loop", c_int32), ("njobs", c_int32),
+                ("jobs", ctypes.POINTER(LoadJob))]
+
+
 P, I, F, U32, U64 = c_void_p, c_int32, c_float, ctypes.c_uint32, ctypes.c_uint64
 PCFG, PST = ctypes.POINTER(EnvConfig), ctypes.POINTER(EnvState)
 
@@ -97,6 +126,17 @@ _PROTOS = {
     "mc_ragged_rollout": (I, [P, P, I, P]),
     "mc_ragged_rollout_prepare": (I, [P, P, I]),
     "mc_ragged_check_error": (I, [P, P]),
+    "mc_server_create": (I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(c_void_p)]),
+    "mc_server_destroy": (I, [P]),
+    "mc_server_job_bytes": (ctypes.c_int64, [PCFG]),
+    "mc_server_admit": (I, [P, PCFG, ctypes.POINTER(c_int32)]),
+    "mc_server_release": (I, [P, I]),
+    "mc_server_job_state": (I, [P, I, PST]),
+    "mc_server_submit": (I, [P, I, I, P, ctypes.POINTER(ctypes.c_int64)]),
+    "mc_server_wait": (I, [P, ctypes.c_int64, P, P, ctypes.c_int64]),
+    "mc_server_get_stats": (I, [P, ctypes.POINTER(ServerStats)]),
+    "mc_server_reset_stats": (I, [P]),
+    "mc_server_drive": (I, [P, ctypes.POINTER(LoadConfig), ctypes.POINTER(ServerStats)]),
     "mc_generate_world": (I, [P, I, I, I, I, I, U32, P]),
     "mc_place_tree": (I, [P, I, I, I, I, I, I, I, P]),
     "mc_place_house": (I, [P, I, I, I, I, I, I, I, P]),

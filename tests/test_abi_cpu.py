@@ -81,3 +81,21 @@ def test_ragged_entry_points_validate_before_launch():
     assert L.mc_ragged_set_config(None, None) == capi.MC_ERR_INVALID
     assert L.mc_ragged_total_envs(None) == -1
     assert L.mc_ragged_destroy(None) == capi.MC_OK
+
+
+def test_server_admission_arithmetic_and_config_checks():
+    L = capi.lib()
+    c = capi.make_config(1000, 16, 16, 16, 32, 32)
+    al = lambda n: (n + 255) // 256 * 256  # noqa: E731
+    state = (al(1000 * 4096) + 2 * al(12000) + 2 * al(4000) + al(1000) + al(4000) + al(1000) + al(20000)
+             + al(1000 * 3072) + al(4000))
+    assert L.mc_server_job_bytes(ctypes.byref(c)) == state + al(4096) + 4096
+    c.world_x = 0
+    assert L.mc_server_job_bytes(ctypes.byref(c)) == -1
+    out = ctypes.c_void_p()
+    bad = capi.ServerConfig(0, 0, 1, 2, 0)  # no budget
+    assert L.mc_server_create(ctypes.byref(bad), ctypes.byref(out)) == capi.MC_ERR_INVALID
+    bad = capi.ServerConfig(1 << 30, 0, 1, 9, 0)  # max_inflight
+    assert L.mc_server_create(ctypes.byref(bad), ctypes.byref(out)) == capi.MC_ERR_INVALID
+    assert "max_inflight" in capi.last_error()
+    assert L.mc_server_destroy(None) == capi.MC_OK
