@@ -41,7 +41,6 @@ sys.path.insert(0, os.path.join(ROOT, "mine.cu_b200"))
 WORKLOAD = dict(workload="peak shape: B=32768 envs/GPU, world 16^3, 32x32x3 uint8 obs (shaded), "
                 "uniform discrete actions seed 1", batch_size=32768, world=16, res=32, obs_dtype="uint8",
                 max_steps=64, seed=1, look_delta=0.1)
-BYTES_PER_ENV_STEP = 16 ** 3 + 32 * 32 * 3  # world read + obs written (algorithmic)
 METRIC = "env-steps/s at B=32K, W=16, 32x32 (fused step, CUDA graph)"
 
 
@@ -135,6 +134,17 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def workload(args):
+    """The peak-shape workload, or the shape --shape B,W,R asks for (profiling runs)."""
+    W = dict(WORKLOAD)
+    if getattr(args, "shape", ""):
+        b, w, r = (int(x) for x in args.shape.split(","))
+        W.update(batch_size=b, world=w, res=r,
+                 workload=f"B={b} envs/GPU, world {w}^3, {r}x{r}x3 uint8 obs (shaded), uniform discrete actions "
+                          f"seed 1")
+    return W
+
+
 def cpu_baseline(seconds=12.0, B=2048):
     """The CPU restatement of the step (oracle/mc_oracle.c, IEEE numerics,
     OpenMP over envs) on this host's cores, on a bounded sample: B envs of
@@ -166,8 +176,9 @@ def run_mine(args):
     from minecu import MineEnv, _C
 
     rank, world, local = dist_setup(args.gpus)
-    W = WORKLOAD
+    W = workload(args)
     B, K, Wm = W["batch_size"], args.steps, args.warmup
+    bytes_per_env_step = W["world"] ** 3 + W["res"] ** 2 * 3
     dev = torch.device("cuda", local)
     env = MineEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
                   device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], numerics="ref_fast",
@@ -252,13 +263,13 @@ def run_mine(args):
     _ = float(h_rew.sum())  # the host reads the results
 
     peak, peak_kind = load_peaks()
-    achieved = BYTES_PER_ENV_STEP * B / (t_fused / K) / 1e9
+    achieved = bytes_per_env_step * B / (t_fused / K) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": t_fused / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
-        "config": {"workload": W["workload"], "global_batch": B * world, "world": "16x16x16",
-                   "render": "32x32x3 uint8", "obs_dtype": W["obs_dtype"], "numerics": "ref_fast",
+        "config": {"workload": W["workload"], "global_batch": B * world, "world": "{0}x{0}x{0}".format(W["world"]),
+                   "render": "{0}x{0}x3 uint8".format(W["res"]), "obs_dtype": W["obs_dtype"], "numerics": "ref_fast",
                    "form": "fused persistent kernel, K-step CUDA graph", "launch": env.launch_config(),
                    "parallelism": f"env-sharded x{world} (no collective)",
                    "trajectory": f"steps {Wm}..{Wm + K - 1} after reset(), every arm",
@@ -273,7 +284,7 @@ def run_mine(args):
                 "path": "MineEnv.step(actions) per step; pinned H2D actions, D2H rewards+dones"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": float(args.traffic_bytes) if args.traffic_bytes else None, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_env_step": BYTES_PER_ENV_STEP,
+                     "algorithmic_bytes_per_env_step": bytes_per_env_step,
                      "kernel": "k_step_fused (avg over the timed region)"},
         "gpu_launches": K,
         "clocks": clk.summary(),
@@ -354,7 +365,10 @@ def run_mine_ragged(args):
     batch = RaggedBatch(envs)
     total = batch.total
     t_tune = time.perf_counter()
-    tuned = autotune.tune_ragged(batch, use_cache=False)
+    if args.no_tune:
+        tuned = {"config": {k: v for k, v in batch.launch_config().items() if k != "smem_bytes"}, "trials": 0}
+    else:
+        tuned = autotune.tune_ragged(batch, use_cache=False)
     t_tune = time.perf_counter() - t_tune
     acts_w = torch.empty((Wm, total), dtype=torch.uint8, device=dev)
     acts_t = torch.empty((K, total), dtype=torch.uint8, device=dev)
@@ -739,6 +753,8 @@ def main():
                     help="peak: B=32768, 16^3, 32x32 (default); ragged: 24,576 envs in 6 groups; "
                          "serve: the env server under Poisson load")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds per offered-load level (serve)")
+    ap.add_argument("--shape", default="", help="peak workload override B,W,R (batch, world edge, resolution)")
+    ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default launch configuration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
