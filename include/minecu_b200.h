@@ -147,6 +147,12 @@ int mc_env_step(mc_env* env, const int8_t* buttons, const float* look, int form,
 int mc_env_step_discrete(mc_env* env, const uint8_t* actions, int form, void* stream);
 /* MineEnv.get_obs / _render (minecu/__init__.py:446-472). */
 int mc_env_render(mc_env* env, void* stream);
+/* Regenerate every world of the env when the device byte *flag is non-zero,
+ * without a host synchronisation: the reference's "any env done -> every
+ * world regenerated" rule (minecu/__init__.py:356-358, 439-441) across the
+ * shards of a batch split over several GPUs, with *flag the all-reduced
+ * any-done byte. */
+int mc_env_regenerate_if(mc_env* env, const uint8_t* flag, void* stream);
 /* K fused steps of discrete actions actions[K,B] captured once in a CUDA
  * graph and replayed; rewards_out / dones_out ([K,B], optional) receive each
  * step's rewards and dones.  The graph is cached per (actions, outputs, K). */

@@ -148,6 +148,7 @@ extern "C" const mc_backend* mc_backend_ieee();
 // numerics-independent kernels (mc_runtime.cu)
 int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s);
 int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s);
+int mc_launch_regen_if(const mc_kp* p, const uint8_t* flag, cudaStream_t s);
 
 // Record an error message for mc_last_error() and return `code`.
 int mc_set_error(int code, const char* msg);

@@ -260,6 +260,21 @@ int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
+namespace {
+__global__ void k_flag_from_byte(int32_t* flags, const uint8_t* flag) {
+    flags[MC_FLAG_ANY_DONE] = *flag ? 1 : 0;
+}
+}  // namespace
+
+// Regeneration conditional on a device byte (copied into the any-done word,
+// which the last CTA of k_regen clears).
+int mc_launch_regen_if(const mc_kp* p, const uint8_t* flag, cudaStream_t s) {
+    k_flag_from_byte<<<1, 1, 0, s>>>(p->flags, flag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    return mc_launch_regen(p, 1, s);
+}
+
 // ---------------------------------------------------------------------------
 // configuration
 // ---------------------------------------------------------------------------
@@ -703,6 +718,13 @@ extern "C" int mc_env_step_discrete(mc_env* e, const uint8_t* actions, int form,
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     if (e->cfg.batch_size && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
     return do_step(e, nullptr, nullptr, actions, form, (cudaStream_t)stream);
+}
+
+extern "C" int mc_env_regenerate_if(mc_env* e, const uint8_t* flag, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (!flag) return fail(MC_ERR_INVALID, "flag is NULL");
+    if (e->cfg.batch_size == 0) return MC_OK;
+    return backend_rc(mc_launch_regen_if(&e->kp, flag, (cudaStream_t)stream), "regen");
 }
 
 extern "C" int mc_env_render(mc_env* e, void* stream) {

@@ -474,6 +474,12 @@ void env_step_discrete(std::shared_ptr<Env> e, torch::Tensor actions, int form) 
 
 void env_render(std::shared_ptr<Env> e) { ck(mc_env_render(e->h, cur_stream()), "render"); }
 
+void env_regenerate_if(std::shared_ptr<Env> e, torch::Tensor flag) {
+    TORCH_CHECK(flag.is_cuda() && flag.numel() >= 1 && flag.element_size() == 1,
+                "flag must be a one-byte CUDA tensor (uint8 or bool)");
+    ck(mc_env_regenerate_if(e->h, static_cast<const uint8_t*>(flag.data_ptr()), cur_stream()), "regenerate_if");
+}
+
 void env_rollout(std::shared_ptr<Env> e, torch::Tensor actions, c10::optional<torch::Tensor> rewards_out,
                  c10::optional<torch::Tensor> dones_out) {
     need(actions, "actions", at::kByte);
@@ -680,6 +686,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("env_step", &env_step);
     m.def("env_step_discrete", &env_step_discrete);
     m.def("env_render", &env_render);
+    m.def("env_regenerate_if", &env_regenerate_if);
     m.def("env_rollout", &env_rollout, py::arg("env"), py::arg("actions"), py::arg("rewards_out") = py::none(),
           py::arg("dones_out") = py::none());
     m.def("env_rollout_prepare", &env_rollout_prepare, py::arg("env"), py::arg("actions"),

@@ -333,6 +333,13 @@ class MineEnv:
             _C.env_render(self._env)
         return self.obs_buffer
 
+    def regenerate_if(self, flag: torch.Tensor) -> None:
+        """Regenerate every world when the one-byte device tensor `flag` is
+        non-zero, with no host synchronisation (the all-reduced any-done
+        flag of a batch sharded over several GPUs; see minecu.shard)."""
+        with torch.cuda.device(self.device):
+            _C.env_regenerate_if(self._env, flag)
+
     def get_obs(self) -> torch.Tensor:
         return self._render()
 

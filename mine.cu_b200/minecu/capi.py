@@ -109,6 +109,7 @@ _PROTOS = {
     "mc_env_step": (I, [P, P, P, ctypes.c_int, P]),
     "mc_env_step_discrete": (I, [P, P, ctypes.c_int, P]),
     "mc_env_render": (I, [P, P]),
+    "mc_env_regenerate_if": (I, [P, P, P]),
     "mc_env_rollout": (I, [P, P, I, P, P, P]),
     "mc_env_rollout_prepare": (I, [P, P, I, P, P]),
     "mc_env_set_fused_config": (I, [P, ctypes.POINTER(FusedConfig)]),

@@ -1,0 +1,88 @@
+"""A batch of envs split over several GPUs, one process per GPU.
+
+Envs are independent, so a global batch of N envs is cut into contiguous
+ranges, one per rank; each rank steps its own MineEnv and nothing crosses
+the ranks in the step itself.  The one coupling the reference has between
+envs - "any env done (or reset) -> every world is regenerated"
+(minecu/__init__.py:290-300, 356-358, 439-441) - would otherwise apply per
+rank only.  With `sync_regen`, after every step (or reset) each rank
+all-reduces a one-byte any-done flag (MAX) and regenerates its worlds when
+the flag is set anywhere, on the device, without a host synchronisation
+(`MineEnv.regenerate_if`).  The result is the same as one MineEnv holding
+the whole batch.  The all-reduce is only needed when episodes can end or
+masked resets happen; a run with neither leaves `sync_regen` off.
+
+Actions for a rank's envs come from the global action stream with the rank's
+first env as the offset (Philox counter = (global env, step)), so the job is
+independent of the number of ranks:
+
+    shard = ShardedEnv(MineEnv(batch_size=count, ...), global_batch=N)
+    _C.philox_actions(acts, shard.start, step0, seed)
+"""
+from __future__ import annotations
+
+from typing import Optional, Tuple
+
+import torch
+import torch.distributed as dist
+
+
+def shard_range(global_batch: int, world: int, rank: int) -> Tuple[int, int]:
+    """(first env, number of envs) of `rank` when `global_batch` envs are cut
+    into `world` contiguous ranges whose sizes differ by at most one."""
+    if world < 1 or not 0 <= rank < world or global_batch < 0:
+        raise ValueError(f"bad shard request: {global_batch} envs, world {world}, rank {rank}")
+    base, extra = divmod(global_batch, world)
+    start = rank * base + min(rank, extra)
+    return start, base + (1 if rank < extra else 0)
+
+
+def max_over_ranks(x: float, device: Optional[torch.device] = None) -> float:
+    """The maximum of a per-rank number (e.g. a timed region) over all ranks."""
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ShardedEnv:
+    """One rank's contiguous slice of a global batch.  `env` holds this
+    rank's envs (its batch size must be the rank's count) and provides
+    step/reset, a `do_reset` bool tensor and `regenerate_if(flag)`."""
+
+    def __init__(self, env, global_batch: int, sync_regen: bool = True, group=None,
+                 flag_device: Optional[torch.device] = None):
+        self.env = env
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self.start, self.count = shard_range(global_batch, self.world, self.rank)
+        n = getattr(env, "batch_size", None)
+        if n is not None and n != self.count:
+            raise ValueError(f"rank {self.rank} holds envs [{self.start}, {self.start + self.count}); "
+                             f"its env has batch_size {n}")
+        self.global_batch = global_batch
+        self.sync_regen = sync_regen and self.world > 1
+        self.flag_device = flag_device if flag_device is not None else getattr(env, "device", torch.device("cpu"))
+        self._flag = torch.zeros(1, dtype=torch.uint8, device=self.flag_device)
+
+    def _sync(self, local_any: torch.Tensor) -> None:
+        self._flag.copy_(local_any.reshape(1).to(device=self.flag_device, dtype=torch.uint8))
+        dist.all_reduce(self._flag, op=dist.ReduceOp.MAX, group=self.group)
+        self.env.regenerate_if(self._flag)
+
+    def step(self, *args):
+        out = self.env.step(*args)
+        if self.sync_regen:
+            self._sync(torch.as_tensor(self.env.do_reset).any())
+        return out
+
+    def reset(self, mask: Optional[torch.Tensor] = None):
+        obs = self.env.reset(mask)
+        if self.sync_regen:
+            local = torch.ones(1, dtype=torch.bool) if mask is None else torch.as_tensor(mask).any()
+            self._sync(local)
+            if mask is not None:
+                obs = self.env.get_obs()  # a world regenerated for another rank changes this rank's view
+        return obs
