@@ -184,16 +184,36 @@ def run_mine(args):
                   device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], numerics="ref_fast",
                   form="fused", look_delta=W["look_delta"])
     if args.launch:
-        st, wpc, cps, ppl = (int(x) for x in args.launch.split(","))
-        env.set_launch_config(st, wpc, cps, ppl)
+        env.set_launch_config(*(int(x) for x in args.launch.split(",")))
     stream = torch.cuda.current_stream()
     # every arm below replays steps [0, Wm) untimed and [Wm, Wm+K) timed of
-    # the same seeded trajectory, starting from reset()
+    # the same seeded trajectory, starting from reset(); with --start-state
+    # every arm instead starts from a saved state at step Wm (profiling runs
+    # of late steps with few launches before the captured one)
+    saved = None
+    if args.start_state and os.path.exists(args.start_state):
+        saved = torch.load(args.start_state, map_location=dev)
+        Wm = int(saved["step"])
     acts_w = torch.empty((Wm, B), dtype=torch.uint8, device=dev)
     acts_t = torch.empty((K, B), dtype=torch.uint8, device=dev)
     _C.philox_actions(acts_w, rank * B, 0, W["seed"])
     _C.philox_actions(acts_t, rank * B, Wm, W["seed"])
-    env.prepare_rollout(acts_w)
+
+    def start(eager=False):
+        """Bring the env to the first timed step of the window."""
+        if saved is not None:
+            env.load_state_dict(saved["state"])
+            return
+        env.reset()
+        if eager:
+            for s in range(Wm):
+                env.step(acts_w[s])
+        else:
+            env.rollout(acts_w)
+        if args.start_state and not os.path.exists(args.start_state):
+            torch.save({"step": Wm, "state": env.state_dict()}, args.start_state)
+    if Wm:
+        env.prepare_rollout(acts_w)
     env.prepare_rollout(acts_t)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -209,8 +229,7 @@ def run_mine(args):
         return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
 
     # ---- fused step, K steps in one CUDA graph (value) ----------------------
-    env.reset()
-    env.rollout(acts_w)
+    start()
     with ClockSampler(local) as clk:
         t_fused = timed(lambda: env.rollout(acts_t))
     env.check_error()
@@ -218,8 +237,7 @@ def run_mine(args):
 
     # ---- same, L2 flushed (a 256 MB write) before every step ----------------
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    env.reset()
-    env.rollout(acts_w)
+    start()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     torch.cuda.synchronize()
@@ -234,9 +252,7 @@ def run_mine(args):
 
     # ---- plain form (the reference's kernel sequence, eager) ---------------
     env.form = "plain"
-    env.reset()
-    for s in range(Wm):
-        env.step(acts_w[s])
+    start(eager=True)
     t_plain = timed(lambda: [env.step(acts_t[s]) for s in range(K)])
     plain_value = B * K * world / t_plain
     env.form = "fused"
@@ -246,10 +262,7 @@ def run_mine(args):
     h_rew = torch.empty((K, B), dtype=torch.float32).pin_memory()
     h_done = torch.empty((K, B), dtype=torch.bool).pin_memory()
     d_act = torch.empty((B,), dtype=torch.uint8, device=dev)
-    env.reset()
-    for s in range(Wm):
-        d_act.copy_(h_acts[s], non_blocking=True)
-        env.step(d_act)
+    start(eager=True)
 
     def e2e_loop():
         for s in range(K):
@@ -273,8 +286,8 @@ def run_mine(args):
                    "form": "fused persistent kernel, K-step CUDA graph", "launch": env.launch_config(),
                    "parallelism": f"env-sharded x{world} (no collective)",
                    "trajectory": f"steps {Wm}..{Wm + K - 1} after reset(), every arm",
-                   "l2": "per-step working set 235 MB (worlds 134 MB + obs 101 MB) > 126 MB L2; no flush "
-                         "(l2_flushed: 256 MB write before every step)"},
+                   "l2": f"per-step working set {bytes_per_env_step * B / 1e6:.0f} MB (worlds + obs); the peak shape's "
+                         "235 MB exceeds the 126 MB L2: no flush (l2_flushed: 256 MB write before every step)"},
         "l2_flushed": {"value": B * K * world / t_flushed, "unit": "env-steps/s",
                        "ms_per_step": t_flushed / K * 1e3},
         "plain": {"value": plain_value, "unit": "env-steps/s", "ms_per_step": t_plain / K * 1e3,
@@ -746,7 +759,9 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,tile_w")
+    ap.add_argument("--launch", default="", help="stage,warps_per_cta,ctas_per_sm,tile_w[,team_warps,coop]")
+    ap.add_argument("--start-state", default="", help="peak: start every arm from this saved state (written "
+                                                      "after the warm-up if it does not exist)")
     ap.add_argument("--traffic-bytes", type=float, default=0.0,
                     help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
     ap.add_argument("--workload", default="peak", choices=["peak", "ragged", "serve"],
