@@ -549,10 +549,18 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // holds air, view_distance > 0 and max_steps >= 1, and for FASTG the eye is
 // at or above the ground) the first loop iteration is known to advance
 // without a hit, so its tests are skipped.
+//
+// With `sky_exit` (per env: `inside`, no ground shortcut, and the caller does
+// not need the face and distance of sky pixels, only their colour) the march stops as soon as
+// the ray leaves the box: voxel coordinates move monotonically, so a ray that
+// left never re-enters, and the reference, which keeps stepping until it is
+// past the exit distance, also ends it as sky.  Only the axis just stepped is
+// bounds-checked.  With `vd_safe` (per env: every in-box voxel is entered
+// closer than view_distance) the distance test is skipped.
 template <bool FASTG, class V>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                          int wz, int max_steps, float vd, int gh, bool inside,
-                                         bool skip_first = false) {
+                                         bool skip_first = false, bool sky_exit = false, bool vd_safe = false) {
     float ray_x, ray_y, ray_z;
     ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::sqrt(len2(ray_x, ray_y, ray_z));
@@ -596,6 +604,72 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
     int step = 0;
+    if (!FASTG && sky_exit && vd_safe) {
+        // The same march with no distance test and no branch per axis: the
+        // reference's if / else-if / else choice of axis (kernels.cu:239-255)
+        // is made with selects, so lanes stepping different axes do not take
+        // turns; one test per iteration ends the loop (hit, left the box, or
+        // max_steps).  The eye's voxel is inside the box.
+        int8_t b = AIR;
+        if (!skip_first && max_steps > 0) b = vox(idx);
+        while (b < 0 && max_steps > 0) {
+            const bool bx = tmx < tmy && tmx < tmz;
+            const bool by = !bx && tmy < tmz;
+            const bool bz = !bx && !by;
+            t = bx ? tmx : (by ? tmy : tmz);
+            const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
+            tmx = bx ? tn : tmx;
+            tmy = by ? tn : tmy;
+            tmz = bz ? tn : tmz;
+            vx += bx ? sx : 0;
+            vy += by ? sy : 0;
+            vz += bz ? sz : 0;
+            idx += bx ? dix : (by ? diy : diz);
+            face = bx ? 0 : (by ? 1 : 2);
+            const bool out = (unsigned)vx >= (unsigned)wx || (unsigned)vy >= (unsigned)wy || (unsigned)vz >= (unsigned)wz;
+            if (out || ++step >= max_steps) break;
+            b = vox(idx);
+        }
+        h.blk = (b >= 0) ? (int)b : AIR;
+        h.face = face;
+        h.t = t;
+        return h;
+    }
+    if (!FASTG && sky_exit) {
+        // the eye's voxel is inside the box.  (Not with the ground shortcut:
+        // a ray the reference keeps stepping after the box can still reach
+        // y < ground_height there.)
+        bool out = false;
+        if (skip_first) {
+            if (tmx < tmy && tmx < tmz) {
+                t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0; out = (unsigned)vx >= (unsigned)wx;
+            } else if (tmy < tmz) {
+                t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1; out = (unsigned)vy >= (unsigned)wy;
+            } else {
+                t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2; out = (unsigned)vz >= (unsigned)wz;
+            }
+            step = 1;
+        }
+        for (; step < max_steps; ++step) {
+            if (!vd_safe && t >= vd) break;
+            if (out) break;  // left the box: sky
+            int8_t b = vox(idx);
+            if (b >= 0) {
+                h.blk = b;
+                break;
+            }
+            if (tmx < tmy && tmx < tmz) {
+                t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0; out = (unsigned)vx >= (unsigned)wx;
+            } else if (tmy < tmz) {
+                t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1; out = (unsigned)vy >= (unsigned)wy;
+            } else {
+                t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2; out = (unsigned)vz >= (unsigned)wz;
+            }
+        }
+        h.face = face;
+        h.t = t;
+        return h;
+    }
     if (skip_first) {
         if (tmx < tmy && tmx < tmz) {
             t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0;
@@ -637,6 +711,17 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
     h.face = face;
     h.t = t;
     return h;
+}
+
+// Every voxel of the box is entered closer than view_distance (with a margin
+// far above the rounding of the DDA's accumulated distances), so the march's
+// distance test cannot end a ray inside the box.
+__device__ __forceinline__ bool box_within_view(const Cam& c, int wx, int wy, int wz, float vd) {
+    const float dx = fmaxf(c.eye_x, (float)wx - c.eye_x);
+    const float dy = fmaxf(c.eye_y, (float)wy - c.eye_y);
+    const float dz = fmaxf(c.eye_z, (float)wz - c.eye_z);
+    const float m = vd - 1.0f;
+    return m > 0.0f && dx * dx + dy * dy + dz * dz < m * m;
 }
 
 __device__ __forceinline__ bool eye_inside(const Cam& c, int wx, int wy, int wz, float vd) {
@@ -1156,10 +1241,11 @@ __device__ __forceinline__ RayPar ray_par(const mc_kp& p) {
 // One pixel's ray through one of the two voxel sources.
 template <int FAM, class V>
 __device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const Dda0& d0, float u, float v,
-                                           const V& vox, bool inside, bool skip_first) {
+                                           const V& vox, bool inside, bool skip_first, bool sky_exit = false,
+                                           bool vd_safe = false) {
     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST)
         return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
-                                                    inside, skip_first);
+                                                    inside, skip_first, sky_exit, vd_safe);
     if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first);
 }
@@ -1396,6 +1482,8 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
         }
         // ---- march every pixel ---------------------------------------------
         const Dda0 d0 = dda0(c);
+        const bool sky_exit = inside && !p.dbg_pixel;
+        const bool vd_safe = sky_exit && box_within_view(c, p.wx, p.wy, p.wz, p.vd);
         const int TW = L.tile_w, TH = L.tile_h;
         const int lx = lane % TW, ly = lane / TW;
         const int bpp = 3 * (F32 ? 4 : 1);  // bytes per pixel
@@ -1408,8 +1496,8 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                     Hit h;
                     const float u = s_u[px];
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
-                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first);
-                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first);
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
+                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
                     } else if (FAM == MC_FAM_FP16) {
                         if (STAGE) h = fp16_ray(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                         else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
