@@ -556,7 +556,8 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // left never re-enters, and the reference, which keeps stepping until it is
 // past the exit distance, also ends it as sky.  Only the axis just stepped is
 // bounds-checked.  With `vd_safe` (per env: every in-box voxel is entered
-// closer than view_distance) the distance test is skipped.
+// closer than view_distance) the march has no distance test and chooses the
+// axis without branches.
 template <bool FASTG, class V>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                          int wz, int max_steps, float vd, int gh, bool inside,
@@ -778,9 +779,13 @@ __device__ __forceinline__ uint32_t to_u8(float x) {
 // Flat ray of render_kernel_uint8_minimal / _prebasis / _smem
 // (kernels.cu:1036-1097, 619-679): rsqrtf normalisation, no AABB, no fog,
 // unsigned bounds test, non-cubic world.
+// With `sky_exit` (per env: the eye's voxel is inside the world, and the
+// caller needs only the colour of sky pixels) the march stops when the ray
+// leaves the box, where the reference keeps stepping out-of-box voxels until
+// max_steps: a ray that left never re-enters, so both end as sky.
 template <bool TRIG, class V>
 __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
-                                        int wz, int max_steps, bool skip_first = false) {
+                                        int wz, int max_steps, bool skip_first = false, bool sky_exit = false) {
     float ray_x, ray_y, ray_z;
     ray_dir<TRIG>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
@@ -807,6 +812,33 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
     int face = -1;
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
+    if (sky_exit) {
+        // branch-free axis choice as in shade_ray; one exit test per iteration
+        int8_t b = AIR;
+        int step = 0;
+        if (!skip_first && max_steps > 0) b = vox(idx);
+        while (b < 0 && max_steps > 0) {
+            const bool bx = tmx < tmy && tmx < tmz;
+            const bool by = !bx && tmy < tmz;
+            const bool bz = !bx && !by;
+            const float tsel = bx ? tmx : (by ? tmy : tmz);
+            const float tn = N::add(tsel, bx ? tdx : (by ? tdy : tdz));
+            tmx = bx ? tn : tmx;
+            tmy = by ? tn : tmy;
+            tmz = bz ? tn : tmz;
+            vx += bx ? sx : 0;
+            vy += by ? sy : 0;
+            vz += bz ? sz : 0;
+            idx += bx ? dix : (by ? diy : diz);
+            face = bx ? 0 : (by ? 1 : 2);
+            const bool out = (unsigned)vx >= (unsigned)wx || (unsigned)vy >= (unsigned)wy || (unsigned)vz >= (unsigned)wz;
+            if (out || ++step >= max_steps) break;
+            b = vox(idx);
+        }
+        h.blk = (b >= 0) ? (int)b : AIR;
+        h.face = face;
+        return h;
+    }
     for (int step = 0; step < max_steps; ++step) {
         // skip_first: the eye's voxel is known to be air or outside the world
         if ((step > 0 || !skip_first) &&
@@ -1247,7 +1279,7 @@ __device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const 
         return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
                                                     inside, skip_first, sky_exit, vd_safe);
     if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
-    return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first);
+    return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
 }
 
 __device__ __forceinline__ void mbar_init_warp(uint32_t mbar_a, int lane) {
@@ -1482,7 +1514,10 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
         }
         // ---- march every pixel ---------------------------------------------
         const Dda0 d0 = dda0(c);
-        const bool sky_exit = inside && !p.dbg_pixel;
+        // per-env facts that let the march stop early (debug output needs the
+        // reference's face and distance of sky pixels too)
+        const bool sky_exit = (FAM == MC_FAM_SHADED) ? (inside && p.vd > 0.0f && !p.dbg_pixel)
+                                                     : (eye_inb && !p.dbg_pixel);
         const bool vd_safe = sky_exit && box_within_view(c, p.wx, p.wy, p.wz, p.vd);
         const int TW = L.tile_w, TH = L.tile_h;
         const int lx = lane % TW, ly = lane / TW;
@@ -1503,8 +1538,8 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                         else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     } else {
                         constexpr bool TRIG = (FAM != MC_FAM_PREBASIS);
-                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first);
-                        else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first);
+                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
+                        else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
                     }
                     const int so = ly * W + px;  // pixel within the staged band
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
@@ -1758,6 +1793,12 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
     uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
     const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
     const bool inside = (r.bits & MC_ER_INSIDE) != 0, skip_first = (r.bits & MC_ER_SKIP) != 0;
+    // per-env facts that let the march stop early (see shade_ray / flat_ray)
+    const bool eye_inb = (unsigned)(int)floorf(r.c.eye_x) < (unsigned)rp.wx &&
+                         (unsigned)(int)floorf(r.c.eye_y) < (unsigned)rp.wy &&
+                         (unsigned)(int)floorf(r.c.eye_z) < (unsigned)rp.wz;
+    const bool sky_exit = (FAM == MC_FAM_SHADED) ? (inside && rp.vd > 0.0f && !dbg_pixel) : (eye_inb && !dbg_pixel);
+    const bool vd_safe = sky_exit && box_within_view(r.c, rp.wx, rp.wy, rp.wz, rp.vd);
     const Dda0 d0 = dda0(r.c);
     const int TW = tile_w, TH = 32 / tile_w;
     const int lx = lane % TW, ly = lane / TW;
@@ -1776,7 +1817,7 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
             const int px = tx0 + lx;
             if (px < W && py < H) {
                 const float u = cx.s_u[px];
-                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first);
+                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe);
                 const int so = ly * W + px;  // pixel within the staged band
                 if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                     float rgb[3];
