@@ -40,8 +40,14 @@ sys.path.insert(0, os.path.join(ROOT, "mine.cu_b200"))
 
 WORKLOAD = dict(workload="peak shape: B=32768 envs/GPU, world 16^3, 32x32x3 uint8 obs (shaded), "
                 "uniform discrete actions seed 1", batch_size=32768, world=16, res=32, obs_dtype="uint8",
-                max_steps=64, seed=1, look_delta=0.1)
+                max_steps=64, seed=1, look_delta=0.1, break_half=False)
+# Render-dominated shape: B=4096, world 32^3, 64x64 uint8, half of the
+# actions forced to "break" (world mutation), seed 2, 500 steps.
+RENDER_WORKLOAD = dict(workload="render-dominated: B=4096 envs/GPU, world 32^3, 64x64x3 uint8 obs (shaded), "
+                       "discrete actions seed 2 with half forced to break", batch_size=4096, world=32, res=64,
+                       obs_dtype="uint8", max_steps=64, seed=2, look_delta=0.1, break_half=True)
 METRIC = "env-steps/s at B=32K, W=16, 32x32 (fused step, CUDA graph)"
+RENDER_METRIC = "env-steps/s at B=4096, W=32, 64x64, half break actions (fused step, CUDA graph)"
 
 
 def load_peaks():
@@ -135,8 +141,8 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 def workload(args):
-    """The peak-shape workload, or the shape --shape B,W,R asks for (profiling runs)."""
-    W = dict(WORKLOAD)
+    """The peak-shape (or render-dominated) workload, or the shape --shape B,W,R asks for (profiling runs)."""
+    W = dict(RENDER_WORKLOAD if getattr(args, "workload", "peak") == "render" else WORKLOAD)
     if getattr(args, "shape", ""):
         b, w, r = (int(x) for x in args.shape.split(","))
         W.update(batch_size=b, world=w, res=r,
@@ -145,18 +151,18 @@ def workload(args):
     return W
 
 
-def cpu_baseline(seconds=12.0, B=2048):
+def cpu_baseline(seconds=12.0, B=2048, W=WORKLOAD):
     """The CPU restatement of the step (oracle/mc_oracle.c, IEEE numerics,
     OpenMP over envs) on this host's cores, on a bounded sample: B envs of
     the same workload stepped until `seconds` have passed."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
-    W = WORKLOAD
     e = O.OracleEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
                     obs_dtype=W["obs_dtype"], max_steps=W["max_steps"], threads=cores)
     e.reset()
-    acts = [O.discrete_to_buttons(O.philox_actions(B, s, W["seed"]), W["look_delta"]) for s in range(64)]
+    acts = [O.discrete_to_buttons(O.philox_actions(B, s, W["seed"], break_half=W["break_half"]), W["look_delta"])
+            for s in range(64)]
     for s in range(3):  # warm-up
         e.step(*acts[s])
     n, t0 = 0, time.perf_counter()
@@ -196,8 +202,8 @@ def run_mine(args):
         Wm = int(saved["step"])
     acts_w = torch.empty((Wm, B), dtype=torch.uint8, device=dev)
     acts_t = torch.empty((K, B), dtype=torch.uint8, device=dev)
-    _C.philox_actions(acts_w, rank * B, 0, W["seed"])
-    _C.philox_actions(acts_t, rank * B, Wm, W["seed"])
+    _C.philox_actions(acts_w, rank * B, 0, W["seed"], W["break_half"])
+    _C.philox_actions(acts_t, rank * B, Wm, W["seed"], W["break_half"])
 
     def start(eager=False):
         """Bring the env to the first timed step of the window."""
@@ -278,7 +284,8 @@ def run_mine(args):
     peak, peak_kind = load_peaks()
     achieved = bytes_per_env_step * B / (t_fused / K) / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "metric": RENDER_METRIC if args.workload == "render" else METRIC, "value": value, "unit": "env-steps/s",
+        "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": t_fused / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
         "config": {"workload": W["workload"], "global_batch": B * world, "world": "{0}x{0}x{0}".format(W["world"]),
@@ -303,7 +310,7 @@ def run_mine(args):
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B=min(2048, B // 2) if B > 1 else 1, W=W)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -507,7 +514,7 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     import ref_driver
-    W = WORKLOAD
+    W = workload(args)
     if not ref_driver.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libminecu_ref.so not built"}))
         return
@@ -519,7 +526,8 @@ def run_reference(args):
     btns = torch.empty((Kr + Wm, B, 8), dtype=torch.int8)
     looks = torch.empty((Kr + Wm, B, 2), dtype=torch.float32)
     for s in range(Kr + Wm):
-        b, l = O.discrete_to_buttons(O.philox_actions(B, s, W["seed"]), W["look_delta"])
+        b, l = O.discrete_to_buttons(O.philox_actions(B, s, W["seed"], break_half=W["break_half"]),
+                                     W["look_delta"])
         btns[s] = torch.from_numpy(b)
         looks[s] = torch.from_numpy(l)
     d_btn, d_look = btns.to(dev), looks.to(dev)
@@ -554,7 +562,8 @@ def run_reference(args):
     te = ev0.elapsed_time(ev1) / 1e3
     e2e = B * Kr / te
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "env-steps/s", "n_gpus": 1, "steps": Kr,
+        "impl": "reference", "metric": RENDER_METRIC if args.workload == "render" else METRIC, "value": value,
+        "unit": "env-steps/s", "n_gpus": 1, "steps": Kr,
         "warmup": Wm, "ms_per_step": t / Kr * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
         "config": {"workload": W["workload"], "global_batch": B, "obs_dtype": W["obs_dtype"],
@@ -764,9 +773,9 @@ def main():
                                                       "after the warm-up if it does not exist)")
     ap.add_argument("--traffic-bytes", type=float, default=0.0,
                     help="DRAM bytes per fused launch from an ncu capture (reported as roofline.traffic)")
-    ap.add_argument("--workload", default="peak", choices=["peak", "ragged", "serve"],
-                    help="peak: B=32768, 16^3, 32x32 (default); ragged: 24,576 envs in 6 groups; "
-                         "serve: the env server under Poisson load")
+    ap.add_argument("--workload", default="peak", choices=["peak", "render", "ragged", "serve"],
+                    help="peak: B=32768, 16^3, 32x32 (default); render: B=4096, 32^3, 64x64, half break "
+                         "actions; ragged: 24,576 envs in 6 groups; serve: the env server under Poisson load")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds per offered-load level (serve)")
     ap.add_argument("--shape", default="", help="peak workload override B,W,R (batch, world edge, resolution)")
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default launch configuration")
@@ -782,7 +791,7 @@ def main():
         else:
             run_reference(args)
     else:
-        {"peak": run_mine, "ragged": run_mine_ragged, "serve": run_mine_serve}[args.workload](args)
+        {"peak": run_mine, "render": run_mine, "ragged": run_mine_ragged, "serve": run_mine_serve}[args.workload](args)
 
 
 if __name__ == "__main__":

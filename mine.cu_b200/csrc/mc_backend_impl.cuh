@@ -613,24 +613,51 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         // max_steps).  The eye's voxel is inside the box.
         int8_t b = AIR;
         if (!skip_first && max_steps > 0) b = vox(idx);
-        while (b < 0 && max_steps > 0) {
-            const bool bx = tmx < tmy && tmx < tmz;
-            const bool by = !bx && tmy < tmz;
-            const bool bz = !bx && !by;
-            t = bx ? tmx : (by ? tmy : tmz);
-            const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
-            tmx = bx ? tn : tmx;
-            tmy = by ? tn : tmy;
-            tmz = bz ? tn : tmz;
-            vx += bx ? sx : 0;
-            vy += by ? sy : 0;
-            vz += bz ? sz : 0;
-            idx += bx ? dix : (by ? diy : diz);
-            face = bx ? 0 : (by ? 1 : 2);
-            const bool out = (unsigned)vx >= (unsigned)wx || (unsigned)vy >= (unsigned)wy || (unsigned)vz >= (unsigned)wz;
-            if (out || ++step >= max_steps) break;
-            b = vox(idx);
+        bool lbx = false, lby = false, adv = false;
+        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? wy - 1 - vy : vy, cz = (sz > 0) ? wz - 1 - vz : vz;
+        if (max_steps > wx + wy + wz) {
+            // every ray leaves the box before max_steps: no step count
+            while (b < 0) {
+                const bool bx = tmx < tmy && tmx < tmz;
+                const bool by = !bx && tmy < tmz;
+                const bool bz = !bx && !by;
+                t = bx ? tmx : (by ? tmy : tmz);
+                const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
+                tmx = bx ? tn : tmx;
+                tmy = by ? tn : tmy;
+                tmz = bz ? tn : tmz;
+                cx -= bx ? 1 : 0;
+                cy -= by ? 1 : 0;
+                cz -= bz ? 1 : 0;
+                idx += bx ? dix : (by ? diy : diz);
+                lbx = bx;
+                lby = by;
+                adv = true;
+                if ((cx | cy | cz) < 0) break;
+                b = vox(idx);
+            }
+        } else {
+            while (b < 0 && max_steps > 0) {
+                const bool bx = tmx < tmy && tmx < tmz;
+                const bool by = !bx && tmy < tmz;
+                const bool bz = !bx && !by;
+                t = bx ? tmx : (by ? tmy : tmz);
+                const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
+                tmx = bx ? tn : tmx;
+                tmy = by ? tn : tmy;
+                tmz = bz ? tn : tmz;
+                cx -= bx ? 1 : 0;
+                cy -= by ? 1 : 0;
+                cz -= bz ? 1 : 0;
+                idx += bx ? dix : (by ? diy : diz);
+                lbx = bx;
+                lby = by;
+                adv = true;
+                if ((cx | cy | cz) < 0 || ++step >= max_steps) break;
+                b = vox(idx);
+            }
         }
+        if (adv) face = lbx ? 0 : (lby ? 1 : 2);
         h.blk = (b >= 0) ? (int)b : AIR;
         h.face = face;
         h.t = t;
