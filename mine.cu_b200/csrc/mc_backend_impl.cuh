@@ -554,11 +554,14 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // not need the face and distance of sky pixels, only their colour) the march stops as soon as
 // the ray leaves the box: voxel coordinates move monotonically, so a ray that
 // left never re-enters, and the reference, which keeps stepping until it is
-// past the exit distance, also ends it as sky.  Only the axis just stepped is
-// bounds-checked.  With `vd_safe` (per env: every in-box voxel is entered
-// closer than view_distance) the march has no distance test and chooses the
-// axis without branches.
-template <bool FASTG, class V>
+// past the exit distance, also ends it as sky.  The axis is then chosen with
+// selects instead of branches, and the box is tracked with per-axis counts of
+// the in-box steps left.  With `vd_safe` (per env: every in-box voxel is
+// entered closer than view_distance) the march has no distance test.
+// VDLIM = false leaves out the branch-free march for view-limited worlds
+// (those then take the reference-shaped loop), for callers whose register
+// budget is better spent elsewhere.
+template <bool FASTG, class V, bool VDLIM = true>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                          int wz, int max_steps, float vd, int gh, bool inside,
                                          bool skip_first = false, bool sky_exit = false, bool vd_safe = false) {
@@ -605,7 +608,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
     int step = 0;
-    if (!FASTG && sky_exit && vd_safe) {
+    if (!FASTG && sky_exit && vd_safe && max_steps > 0) {
         // The same march with no distance test and no branch per axis: the
         // reference's if / else-if / else choice of axis (kernels.cu:239-255)
         // is made with selects, so lanes stepping different axes do not take
@@ -663,37 +666,35 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         h.t = t;
         return h;
     }
-    if (!FASTG && sky_exit) {
-        // the eye's voxel is inside the box.  (Not with the ground shortcut:
-        // a ray the reference keeps stepping after the box can still reach
-        // y < ground_height there.)
-        bool out = false;
-        if (skip_first) {
-            if (tmx < tmy && tmx < tmz) {
-                t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0; out = (unsigned)vx >= (unsigned)wx;
-            } else if (tmy < tmz) {
-                t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1; out = (unsigned)vy >= (unsigned)wy;
-            } else {
-                t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2; out = (unsigned)vz >= (unsigned)wz;
-            }
-            step = 1;
+    if (VDLIM && !FASTG && sky_exit && max_steps > 0) {
+        // the same branch-free march with the distance test and the step
+        // count in its single exit test (worlds whose far corners lie beyond
+        // view_distance)
+        int8_t b = AIR;
+        if (!skip_first) b = vox(idx);
+        bool lbx = false, lby = false, adv = false;
+        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? wy - 1 - vy : vy, cz = (sz > 0) ? wz - 1 - vz : vz;
+        while (b < 0) {
+            const bool bx = tmx < tmy && tmx < tmz;
+            const bool by = !bx && tmy < tmz;
+            const bool bz = !bx && !by;
+            t = bx ? tmx : (by ? tmy : tmz);
+            const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
+            tmx = bx ? tn : tmx;
+            tmy = by ? tn : tmy;
+            tmz = bz ? tn : tmz;
+            cx -= bx ? 1 : 0;
+            cy -= by ? 1 : 0;
+            cz -= bz ? 1 : 0;
+            idx += bx ? dix : (by ? diy : diz);
+            lbx = bx;
+            lby = by;
+            adv = true;
+            if ((cx | cy | cz) < 0 || ++step >= max_steps || t >= vd) break;
+            b = vox(idx);
         }
-        for (; step < max_steps; ++step) {
-            if (!vd_safe && t >= vd) break;
-            if (out) break;  // left the box: sky
-            int8_t b = vox(idx);
-            if (b >= 0) {
-                h.blk = b;
-                break;
-            }
-            if (tmx < tmy && tmx < tmz) {
-                t = tmx; tmx = N::add(tmx, tdx); vx += sx; idx += dix; face = 0; out = (unsigned)vx >= (unsigned)wx;
-            } else if (tmy < tmz) {
-                t = tmy; tmy = N::add(tmy, tdy); vy += sy; idx += diy; face = 1; out = (unsigned)vy >= (unsigned)wy;
-            } else {
-                t = tmz; tmz = N::add(tmz, tdz); vz += sz; idx += diz; face = 2; out = (unsigned)vz >= (unsigned)wz;
-            }
-        }
+        if (adv) face = lbx ? 0 : (lby ? 1 : 2);
+        h.blk = (b >= 0) ? (int)b : AIR;
         h.face = face;
         h.t = t;
         return h;
@@ -1558,8 +1559,10 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                     Hit h;
                     const float u = s_u[px];
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
-                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
-                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
+                        // the one-warp-per-env kernel keeps its 64-register budget: the
+                        // branch-free march only where the whole box is within view
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxShared, false>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
+                        else h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxGlobal, false>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
                     } else if (FAM == MC_FAM_FP16) {
                         if (STAGE) h = fp16_ray(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                         else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
