@@ -15,6 +15,9 @@
 //  * the completer waits for those events in launch order, hands the
 //    results to the requests and records their latency (submission to
 //    results in host memory).
+// Both threads poll (the launcher its queue for a while before sleeping, the
+// completer its event) instead of blocking, which keeps thread wake-ups out
+// of the request latency at the cost of two busy host cores under load.
 // Up to max_inflight launches are queued on the device at once, so the host
 // work of the next launch overlaps the current one.  A job's requests run in
 // submission order (one stream).  With batching = 0 the launcher takes one
@@ -25,6 +28,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -46,6 +50,7 @@ using Clock = std::chrono::steady_clock;
 constexpr int kMaxSlots = 4;
 constexpr long long kDefaultCap = 1LL << 20;
 constexpr int64_t kJobOverhead = 4096;  // flag words and handle-side allocations
+constexpr int kSpin = 20000;            // launcher polls before sleeping on the condition variable
 
 struct Job;
 
@@ -83,6 +88,7 @@ struct Slot {
     uint8_t* d_res = nullptr;
     std::vector<Req*> reqs;
     std::vector<long long> offs;  // env offset of each step request in the launch
+    long long total = 0;          // envs of the step launch: rewards at [0, 4 total), dones after them
     bool step_launch = false;
     bool busy = false;
 };
@@ -172,6 +178,8 @@ struct mc_server {
     std::unordered_map<int64_t, Req*> tickets;
     int64_t next_ticket = 1;
     int pending = 0;  // requests queued or in flight
+    std::atomic<int> queued{0};  // requests queued, not launched (read without the lock by the launcher's spin)
+    std::atomic<bool> stopping{false};
     bool stop = false, launcher_done = false;
     std::thread launcher, completer;
     cudaStream_t stream = nullptr, admit_stream = nullptr;
@@ -230,6 +238,7 @@ std::vector<Req*> take_batch(mc_server* s) {
         r->job->queue.pop_front();
         r->job->inflight++;
     }
+    s->queued -= (int)out.size();
     return out;
 }
 
@@ -256,8 +265,10 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
         }
         cudaError_t ce = cudaMemcpyAsync(sl.d_act, sl.h_act, (size_t)off, cudaMemcpyHostToDevice, st);
         if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: actions upload");
+        // rewards then dones, contiguous: one read-back
+        sl.total = off;
         float* d_rew = reinterpret_cast<float*>(sl.d_res);
-        uint8_t* d_done = sl.d_res + s->cap * 4;
+        uint8_t* d_done = sl.d_res + off * 4;
         if (s->cfg.batching) {
             const int G = (int)steps.size();
             std::vector<const mc_kp*> kps(G);
@@ -298,9 +309,7 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
                 ce = cudaMemcpyAsync(d_done, r->job->st.do_reset, B, cudaMemcpyDeviceToDevice, st);
             if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: result gather");
         }
-        ce = cudaMemcpyAsync(sl.h_res, sl.d_res, (size_t)off * 4, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess)
-            ce = cudaMemcpyAsync(sl.h_res + s->cap * 4, d_done, (size_t)off, cudaMemcpyDeviceToHost, st);
+        ce = cudaMemcpyAsync(sl.h_res, sl.d_res, (size_t)off * 5, cudaMemcpyDeviceToHost, st);
         if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: results read-back");
     }
     return rc;
@@ -311,6 +320,12 @@ void launcher_main(mc_server* s) {
     for (;;) {
         std::vector<Req*> reqs;
         int si;
+        // poll for work for a while before sleeping: a thread woken through
+        // the condition variable adds tens of microseconds to a request
+        for (int i = 0; i < kSpin && s->queued.load(std::memory_order_relaxed) == 0 &&
+                        !s->stopping.load(std::memory_order_relaxed);
+             ++i)
+            std::this_thread::yield();
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || has_queued(s); });
@@ -348,7 +363,9 @@ void completer_main(mc_server* s) {
             si = s->flight.front();
         }
         Slot& sl = s->slots[si];
-        cudaError_t ce = cudaEventSynchronize(sl.ev);
+        // poll the event rather than block on it (lower completion latency)
+        cudaError_t ce;
+        while ((ce = cudaEventQuery(sl.ev)) == cudaErrorNotReady) std::this_thread::yield();
         const Clock::time_point t = Clock::now();
         std::lock_guard<std::mutex> lk(s->mu);
         int nsteps = 0;
@@ -360,7 +377,7 @@ void completer_main(mc_server* s) {
                 ++nsteps;
                 if (!r->detached && r->status == MC_OK) {
                     const float* rew = reinterpret_cast<const float*>(sl.h_res) + sl.offs[i];
-                    const uint8_t* dn = sl.h_res + s->cap * 4 + sl.offs[i];
+                    const uint8_t* dn = sl.h_res + sl.total * 4 + sl.offs[i];
                     r->rewards.assign(rew, rew + B);
                     r->dones.assign(dn, dn + B);
                 }
@@ -422,6 +439,7 @@ int submit_impl(mc_server* s, int32_t job, int32_t kind, const uint8_t* actions,
     if (ticket) *ticket = detached ? 0 : r->ticket;
     j->queue.push_back(r);
     s->pending++;
+    s->queued++;
     s->cv_work.notify_one();
     return MC_OK;
 }
@@ -520,6 +538,7 @@ extern "C" int mc_server_destroy(mc_server* s) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
+        s->stopping = true;
         s->cv_work.notify_all();
         s->cv_flight.notify_all();
     }
