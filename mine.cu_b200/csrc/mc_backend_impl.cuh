@@ -1328,6 +1328,14 @@ __device__ __forceinline__ void finish_dynamic(int32_t* flags, long long total_w
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fused step, one warp per env (one env group per launch)
+// ---------------------------------------------------------------------------
+// The per-env body below does what agent_step + fill_env + render_env of the
+// team kernel do, written out in one piece: built from those helpers, the
+// same kernel needed spill slots at its 64-register budget (4 CTAs of 8 warps
+// per SM) and ran 8% slower on B=32768, 16^3, 32x32, so it keeps its own
+// copy; the parity tests hold the two kernels to the same bits.
 #ifndef MC_FUSED_MIN_BLOCKS
 #define MC_FUSED_MIN_BLOCKS 4
 #endif
