@@ -618,8 +618,16 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         if (!skip_first && max_steps > 0) b = vox(idx);
         bool lbx = false, lby = false, adv = false;
         int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? wy - 1 - vy : vy, cz = (sz > 0) ? wz - 1 - vz : vz;
-        if (max_steps > wx + wy + wz) {
-            // every ray leaves the box before max_steps: no step count
+        if (max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
+            // every ray leaves the box before max_steps: no step count.  The
+            // voxel index and the three in-box counts share one register:
+            // bits 18.. the index, three 6-bit fields below it counting up
+            // from 31 - (steps left) to 32, whose bit 5 marks leaving the
+            // box; one add moves both, one mask tests the exit.
+            const int fx = 31 - cx, fy = 31 - cy, fz = 31 - cz;
+            int packed = (idx << 18) | (fx << 12) | (fy << 6) | fz;
+            const int px = (dix << 18) + (1 << 12), py = (diy << 18) + (1 << 6), pz = (diz << 18) + 1;
+            constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
             while (b < 0) {
                 const bool bx = tmx < tmy && tmx < tmz;
                 const bool by = !bx && tmy < tmz;
@@ -629,15 +637,12 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 tmx = bx ? tn : tmx;
                 tmy = by ? tn : tmy;
                 tmz = bz ? tn : tmz;
-                cx -= bx ? 1 : 0;
-                cy -= by ? 1 : 0;
-                cz -= bz ? 1 : 0;
-                idx += bx ? dix : (by ? diy : diz);
+                packed += bx ? px : (by ? py : pz);
                 lbx = bx;
                 lby = by;
                 adv = true;
-                if ((cx | cy | cz) < 0) break;
-                b = vox(idx);
+                if (packed & kGuard) break;
+                b = vox(packed >> 18);
             }
         } else {
             while (b < 0 && max_steps > 0) {
