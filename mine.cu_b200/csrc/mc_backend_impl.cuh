@@ -633,10 +633,12 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 const bool by = !bx && tmy < tmz;
                 const bool bz = !bx && !by;
                 t = bx ? tmx : (by ? tmy : tmz);
-                const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
-                tmx = bx ? tn : tmx;
-                tmy = by ? tn : tmy;
-                tmz = bz ? tn : tmz;
+                // three adds (FMA pipe) instead of selecting the delta (ALU pipe,
+                // the busier one); only the chosen axis keeps its sum
+                const float nx = N::add(tmx, tdx), ny = N::add(tmy, tdy), nz = N::add(tmz, tdz);
+                tmx = bx ? nx : tmx;
+                tmy = by ? ny : tmy;
+                tmz = bz ? nz : tmz;
                 packed += bx ? px : (by ? py : pz);
                 lbx = bx;
                 lby = by;
