@@ -652,10 +652,10 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 const bool by = !bx && tmy < tmz;
                 const bool bz = !bx && !by;
                 t = bx ? tmx : (by ? tmy : tmz);
-                const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
-                tmx = bx ? tn : tmx;
-                tmy = by ? tn : tmy;
-                tmz = bz ? tn : tmz;
+                const float nx = N::add(tmx, tdx), ny = N::add(tmy, tdy), nz = N::add(tmz, tdz);
+                tmx = bx ? nx : tmx;
+                tmy = by ? ny : tmy;
+                tmz = bz ? nz : tmz;
                 cx -= bx ? 1 : 0;
                 cy -= by ? 1 : 0;
                 cz -= bz ? 1 : 0;
@@ -686,10 +686,10 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             const bool by = !bx && tmy < tmz;
             const bool bz = !bx && !by;
             t = bx ? tmx : (by ? tmy : tmz);
-            const float tn = N::add(t, bx ? tdx : (by ? tdy : tdz));
-            tmx = bx ? tn : tmx;
-            tmy = by ? tn : tmy;
-            tmz = bz ? tn : tmz;
+            const float nx = N::add(tmx, tdx), ny = N::add(tmy, tdy), nz = N::add(tmz, tdz);
+            tmx = bx ? nx : tmx;
+            tmy = by ? ny : tmy;
+            tmz = bz ? nz : tmz;
             cx -= bx ? 1 : 0;
             cy -= by ? 1 : 0;
             cz -= bz ? 1 : 0;
@@ -856,11 +856,10 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
             const bool bx = tmx < tmy && tmx < tmz;
             const bool by = !bx && tmy < tmz;
             const bool bz = !bx && !by;
-            const float tsel = bx ? tmx : (by ? tmy : tmz);
-            const float tn = N::add(tsel, bx ? tdx : (by ? tdy : tdz));
-            tmx = bx ? tn : tmx;
-            tmy = by ? tn : tmy;
-            tmz = bz ? tn : tmz;
+            const float nx = N::add(tmx, tdx), ny = N::add(tmy, tdy), nz = N::add(tmz, tdz);
+            tmx = bx ? nx : tmx;
+            tmy = by ? ny : tmy;
+            tmz = bz ? nz : tmz;
             vx += bx ? sx : 0;
             vy += by ? sy : 0;
             vz += bz ? sz : 0;
