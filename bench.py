@@ -48,6 +48,13 @@ RENDER_WORKLOAD = dict(workload="render-dominated: B=4096 envs/GPU, world 32^3, 
                        obs_dtype="uint8", max_steps=64, seed=2, look_delta=0.1, break_half=True)
 METRIC = "env-steps/s at B=32K, W=16, 32x32 (fused step, CUDA graph)"
 RENDER_METRIC = "env-steps/s at B=4096, W=32, 64x64, half break actions (fused step, CUDA graph)"
+# DRAM bytes (read + written) of one launch of the workload's step kernel,
+# from the ncu captures summarised in profiles/ (cold caches under ncu)
+TRAFFIC = {
+    "peak": (113.1e6 + 57.5e6, "k_step_fused, step 701, profiles/k_step_fused_peak_late_full.md"),
+    "render": (135.5e6 + 27.2e6, "k_step_team, step 301, profiles/k_step_team_B4096_w32_r64_full.md"),
+    "ragged": (64.0e6 + 14.4e6, "k_step_team, mean of steps 0..14, profiles/k_step_team_ragged_launches.md"),
+}
 
 
 def load_peaks():
@@ -303,7 +310,10 @@ def run_mine(args):
                 "d2h_bytes_per_step": B * 4 + B,
                 "path": "MineEnv.step(actions) per step; pinned H2D actions, D2H rewards+dones"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": float(args.traffic_bytes) if args.traffic_bytes else None, "peak_kind": peak_kind,
+                     "traffic": float(args.traffic_bytes) if args.traffic_bytes else
+                     (TRAFFIC[args.workload][0] if not args.shape else None),
+                     "traffic_source": "--traffic-bytes" if args.traffic_bytes else
+                     (TRAFFIC[args.workload][1] if not args.shape else None), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_env_step": bytes_per_env_step,
                      "kernel": "k_step_fused (avg over the timed region)"},
         "gpu_launches": K,
@@ -488,8 +498,9 @@ def run_mine_ragged(args):
                 "d2h_bytes_per_step": total * 5,
                 "path": "RaggedBatch.step(actions); pinned H2D actions, D2H rewards+dones"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_step": bps,
-                     "kernel": "k_step_ragged (avg over the timed region)"},
+                     "traffic": TRAFFIC["ragged"][0], "traffic_source": TRAFFIC["ragged"][1], "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_step": bps,
+                     "kernel": "k_step_team (avg over the timed region)"},
         "gpu_launches": K * (1 + sum(1 for e in envs if e.episode_length)),
         "clocks": clk.summary(),
     }
