@@ -557,14 +557,17 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // past the exit distance, also ends it as sky.  The axis is then chosen with
 // selects instead of branches, and the box is tracked with per-axis counts of
 // the in-box steps left.  With `vd_safe` (per env: every in-box voxel is
-// entered closer than view_distance) the march has no distance test.
+// entered closer than view_distance) the march has no distance test; there
+// `ytop` (per env: no solid voxel above this y) also ends rays going up once
+// they pass it, as sky.
 // VDLIM = false leaves out the branch-free march for view-limited worlds
 // (those then take the reference-shaped loop), for callers whose register
 // budget is better spent elsewhere.
 template <bool FASTG, class V, bool VDLIM = true>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                          int wz, int max_steps, float vd, int gh, bool inside,
-                                         bool skip_first = false, bool sky_exit = false, bool vd_safe = false) {
+                                         bool skip_first = false, bool sky_exit = false, bool vd_safe = false,
+                                         int ytop = 1 << 20) {
     float ray_x, ray_y, ray_z;
     ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::sqrt(len2(ray_x, ray_y, ray_z));
@@ -617,14 +620,16 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         int8_t b = AIR;
         if (!skip_first && max_steps > 0) b = vox(idx);
         bool lbx = false, lby = false, adv = false;
-        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? wy - 1 - vy : vy, cz = (sz > 0) ? wz - 1 - vz : vz;
+        // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+            cz = (sz > 0) ? wz - 1 - vz : vz;
         if (max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
             // every ray leaves the box before max_steps: no step count.  The
             // voxel index and the three in-box counts share one register:
             // bits 18.. the index, three 6-bit fields below it counting up
             // from 31 - (steps left) to 32, whose bit 5 marks leaving the
             // box; one add moves both, one mask tests the exit.
-            const int fx = 31 - cx, fy = 31 - cy, fz = 31 - cz;
+            const int fx = 31 - cx, fy = 31 - max(cy, -32), fz = 31 - cz;
             int packed = (idx << 18) | (fx << 12) | (fy << 6) | fz;
             const int px = (dix << 18) + (1 << 12), py = (diy << 18) + (1 << 6), pz = (diz << 18) + 1;
             constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
@@ -1531,6 +1536,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
         }
         // ---- stage the world into shared memory ----------------------------
         const int8_t* wsrc = gw;
+        int ytop = p.wy - 1;  // highest layer with a solid voxel (all layers unless measured)
         if (STAGE) {
             if (lane == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1553,6 +1559,22 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
             if (lane == 0 && mod_idx >= 0) sworld[mod_idx] = mod_val;
             __syncwarp();
             wsrc = sworld;
+            // highest layer holding a solid voxel (solid = byte >= 0, sign bit clear)
+            const int layer = p.wx * p.wz;
+            if ((layer & 15) == 0) {
+                const uint4* w4 = reinterpret_cast<const uint4*>(sworld);
+                const int n16 = wxyz >> 4, per_layer = layer >> 4;
+                int top = -1;
+                for (int k = n16 - 1 - lane; k >= 0; k -= 32) {
+                    const uint4 q = w4[k];
+                    const uint32_t solid = (~q.x | ~q.y | ~q.z | ~q.w) & 0x80808080u;
+                    if (solid) {
+                        top = max(top, k / per_layer);
+                        break;  // lower chunks of this lane are lower layers
+                    }
+                }
+                ytop = __reduce_max_sync(0xffffffffu, top);
+            }
         }
         // ---- march every pixel ---------------------------------------------
         const Dda0 d0 = dda0(c);
@@ -1575,7 +1597,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         // the one-warp-per-env kernel keeps its 64-register budget: the
                         // branch-free march only where the whole box is within view
-                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxShared, false>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxShared, false>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe, ytop);
                         else h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxGlobal, false>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
                     } else if (FAM == MC_FAM_FP16) {
                         if (STAGE) h = fp16_ray(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
