@@ -557,9 +557,9 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // past the exit distance, also ends it as sky.  The axis is then chosen with
 // selects instead of branches, and the box is tracked with per-axis counts of
 // the in-box steps left.  With `vd_safe` (per env: every in-box voxel is
-// entered closer than view_distance) the march has no distance test; there
-// `ytop` (per env: no solid voxel above this y) also ends rays going up once
-// they pass it, as sky.
+// entered closer than view_distance) the march has no distance test.  In
+// both, `ytop` (per env: no solid voxel above this layer) ends rays going up
+// once they pass it, as sky.
 // VDLIM = false leaves out the branch-free march for view-limited worlds
 // (those then take the reference-shaped loop), for callers whose register
 // budget is better spent elsewhere.
@@ -685,7 +685,9 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         int8_t b = AIR;
         if (!skip_first) b = vox(idx);
         bool lbx = false, lby = false, adv = false;
-        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? wy - 1 - vy : vy, cz = (sz > 0) ? wz - 1 - vz : vz;
+        // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+        int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+            cz = (sz > 0) ? wz - 1 - vz : vz;
         while (b < 0) {
             const bool bx = tmx < tmy && tmx < tmz;
             const bool by = !bx && tmy < tmz;
@@ -1313,10 +1315,10 @@ __device__ __forceinline__ RayPar ray_par(const mc_kp& p) {
 template <int FAM, class V>
 __device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const Dda0& d0, float u, float v,
                                            const V& vox, bool inside, bool skip_first, bool sky_exit = false,
-                                           bool vd_safe = false) {
+                                           bool vd_safe = false, int ytop = 1 << 20) {
     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST)
         return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
-                                                    inside, skip_first, sky_exit, vd_safe);
+                                                    inside, skip_first, sky_exit, vd_safe, ytop);
     if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
 }
@@ -1337,6 +1339,25 @@ __device__ __forceinline__ void finish_dynamic(int32_t* flags, long long total_w
         flags[MC_FLAG_WARPS_DONE] = 0;
         __threadfence();
     }
+}
+
+// Highest layer of a staged world holding a solid voxel (solid = byte >= 0,
+// sign bit clear), found by one warp; -1 for an empty world; wy - 1 when the
+// layer size is not a multiple of 16 bytes (not measured).
+__device__ __forceinline__ int staged_top_layer(const int8_t* world, int wx, int wy, int wz, int lane) {
+    const int layer = wx * wz;
+    if (layer & 15) return wy - 1;
+    const uint4* w4 = reinterpret_cast<const uint4*>(world);
+    const int n16 = (layer * wy) >> 4, per_layer = layer >> 4;
+    int top = -1;
+    for (int k = n16 - 1 - lane; k >= 0; k -= 32) {
+        const uint4 q = w4[k];
+        if ((~q.x | ~q.y | ~q.z | ~q.w) & 0x80808080u) {
+            top = k / per_layer;
+            break;  // this lane's remaining chunks lie in lower layers
+        }
+    }
+    return __reduce_max_sync(0xffffffffu, top);
 }
 
 // ---------------------------------------------------------------------------
@@ -1559,22 +1580,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
             if (lane == 0 && mod_idx >= 0) sworld[mod_idx] = mod_val;
             __syncwarp();
             wsrc = sworld;
-            // highest layer holding a solid voxel (solid = byte >= 0, sign bit clear)
-            const int layer = p.wx * p.wz;
-            if ((layer & 15) == 0) {
-                const uint4* w4 = reinterpret_cast<const uint4*>(sworld);
-                const int n16 = wxyz >> 4, per_layer = layer >> 4;
-                int top = -1;
-                for (int k = n16 - 1 - lane; k >= 0; k -= 32) {
-                    const uint4 q = w4[k];
-                    const uint32_t solid = (~q.x | ~q.y | ~q.z | ~q.w) & 0x80808080u;
-                    if (solid) {
-                        top = max(top, k / per_layer);
-                        break;  // lower chunks of this lane are lower layers
-                    }
-                }
-                ytop = __reduce_max_sync(0xffffffffu, top);
-            }
+            ytop = staged_top_layer(sworld, p.wx, p.wy, p.wz, lane);
         }
         // ---- march every pixel ---------------------------------------------
         const Dda0 d0 = dda0(c);
@@ -1683,7 +1689,10 @@ struct EnvRender {
     int fill_blk;  // block of the uniform fill of a buried camera
     int mod_idx;   // voxel index the interaction wrote, -1 if none
     int mod_val;
+    int ytop;      // no solid voxel above this layer (wy - 1 unless measured)
 };
+
+
 enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
 
 struct TeamShared {
@@ -1772,6 +1781,7 @@ __device__ __forceinline__ EnvRender agent_step(const mc_kp& p, const ActionSrc&
     r.fill_blk = fill_blk;
     r.mod_idx = mod_idx;
     r.mod_val = mod_val;
+    r.ytop = p.wy - 1;
     return r;
 }
 
@@ -1883,7 +1893,7 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
             const int px = tx0 + lx;
             if (px < W && py < H) {
                 const float u = cx.s_u[px];
-                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe);
+                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe, r.ytop);
                 const int so = ly * W + px;  // pixel within the staged band
                 if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                     float rgb[3];
@@ -2029,6 +2039,8 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                 if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane)) {
                     // the interaction may have written after the copy read the byte
                     if (lane == 0 && r.mod_idx >= 0) world[r.mod_idx] = (int8_t)r.mod_val;
+                    __syncwarp();
+                    r.ytop = staged_top_layer(world, p.wx, p.wy, p.wz, lane);
                 } else {
                     if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
                     warp_no_stage = true;  // the copy may still land: render from global memory from now on
