@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
+#include <type_traits>
 #include "mc_internal.h"
 #include "mc_ieee_math.h"
 #include "mc_philox.h"
@@ -526,6 +527,63 @@ struct Hit {
     int step_y; // sign of the ray's y (shaded shade rule)
 };
 
+#if MC_NUMERICS_FAST
+#define MC_PTX_FTZ ".ftz"
+#else
+#define MC_PTX_FTZ ""
+#endif
+
+// Packed march over a world staged in shared memory (the packed form of
+// shade_ray's branch-free march).  `packed` holds the voxel index in bits
+// 18.. and three 6-bit in-box step counts that set bit 5 of their field when
+// the ray leaves the box; p{x,y,z} move index and count of one axis.  Per
+// iteration the axis of the reference's if / else-if / else choice
+// (kernels.cu:239-255) is three compares whose predicates guard the index
+// and distance updates directly (no selects), and the distance update comes
+// after the voxel test, so at a hit tm still holds the entry distances the
+// choice was made from: the caller recovers the axis and the distance t
+// from them once per ray instead of carrying them through the loop.
+// Returns the block hit (>= 0), or -1 when the ray left the box.
+__device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, int px, int py, int pz, float& tmx,
+                                                   float& tmy, float& tmz, float tdx, float tdy, float tdz) {
+    constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
+    int b;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
+        ".reg .b32 ra;\n\t"
+        ".reg .s32 rv;\n\t"
+        "mov.b32 %0, -1;\n\t"
+        "MC_MARCH_LOOP:\n\t"
+        "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pby|pzy, %2, %3, pna;\n\t"
+        "or.pred pz, pzx, pzy;\n\t"
+        "@pbx add.s32 %4, %4, %5;\n\t"
+        "@pby add.s32 %4, %4, %6;\n\t"
+        "@pz add.s32 %4, %4, %7;\n\t"
+        "and.b32 ra, %4, %8;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "@pq bra MC_MARCH_DONE;\n\t"
+        "shr.s32 ra, %4, 18;\n\t"
+        "add.s32 ra, ra, %9;\n\t"
+        "ld.shared.s8 rv, [ra];\n\t"
+        "setp.ge.s32 pq, rv, 0;\n\t"
+        "@pq bra MC_MARCH_HIT;\n\t"
+        "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %10;\n\t"
+        "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %11;\n\t"
+        "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %12;\n\t"
+        "bra MC_MARCH_LOOP;\n\t"
+        "MC_MARCH_HIT:\n\t"
+        "mov.b32 %0, rv;\n\t"
+        "MC_MARCH_DONE:\n\t"
+        "}"
+        : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(packed)
+        : "r"(px), "r"(py), "r"(pz), "n"(kGuard), "r"(world), "f"(tdx), "f"(tdy), "f"(tdz)
+        : "memory");
+    return b;
+}
+
 // ray_intersects_aabb (kernels.cu:51-79) exit distance for a box [0, ws]^3
 // given the precomputed numerators (0 - eye) and (ws - eye).
 __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float lo_x, float hi_x,
@@ -633,6 +691,22 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             int packed = (idx << 18) | (fx << 12) | (fy << 6) | fz;
             const int px = (dix << 18) + (1 << 12), py = (diy << 18) + (1 << 6), pz = (diz << 18) + 1;
             constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
+            if constexpr (std::is_same<V, VoxShared>::value) {
+                if (b < 0) {
+                    b = (int8_t)march_packed_shared((uint32_t)__cvta_generic_to_shared(vox.w), packed, px, py, pz,
+                                                    tmx, tmy, tmz, tdx, tdy, tdz);
+                    if (b >= 0) {
+                        const bool bx = tmx < tmy && tmx < tmz;
+                        const bool by = !bx && tmy < tmz;
+                        t = bx ? tmx : (by ? tmy : tmz);
+                        face = bx ? 0 : (by ? 1 : 2);
+                    }
+                }
+                h.blk = (b >= 0) ? (int)b : AIR;
+                h.face = face;
+                h.t = t;
+                return h;
+            }
             while (b < 0) {
                 const bool bx = tmx < tmy && tmx < tmz;
                 const bool by = !bx && tmy < tmz;
