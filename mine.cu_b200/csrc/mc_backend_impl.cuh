@@ -519,6 +519,13 @@ struct VoxShared {
     const int8_t* w;
     __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
 };
+// Either source behind one generic pointer (one call site for both), with a
+// per-env flag telling whether it points into shared memory.
+struct VoxEither {
+    const int8_t* w;
+    bool smem;
+    __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+};
 
 struct Hit {
     int blk;    // block id, -1 for sky
@@ -580,6 +587,65 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
         "}"
         : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(packed)
         : "r"(px), "r"(py), "r"(pz), "n"(kGuard), "r"(world), "f"(tdx), "f"(tdy), "f"(tdz)
+        : "memory");
+    return b;
+}
+
+// Counts of the split march: three 7-bit in-box step counts (z bits 0-6,
+// x 7-13, y 14-20) that count up from 63 - (steps left) and set bit 6 of
+// their field on leaving the box, and a 9-bit step count (bits 21-29) that
+// sets its bit 8 when max_steps voxels have been stepped.  A count that
+// starts at or above 64 (y of a ray going up from above `ytop`) ends the ray at
+// its first step; clamping it to 126 keeps the carry out of the field.
+constexpr int kSplitGuard = (1 << 6) | (1 << 13) | (1 << 20) | (1 << 29);
+__device__ __forceinline__ int split_counts(int cx, int cy, int cz, int max_steps, int wx, int wy, int wz) {
+    const int s0 = (max_steps > wx + wy + wz) ? 0 : 256 - max_steps;  // no ray takes more than wx+wy+wz steps
+    return (63 - cz) | ((63 - cx) << 7) | ((63 - max(cy, -63)) << 14) | (s0 << 21);
+}
+
+// The march over a staged world of up to 64 voxels a side, any max_steps:
+// the voxel's shared-memory address moves in one register and the counts
+// (split_counts) in another, so a single mask tests every exit and the load
+// needs no index arithmetic.  Axis choice, predicated updates and the
+// distances left at a hit as in march_packed_shared.  Returns the block hit
+// (>= 0), or -1 when the ray left the box or ran out of steps.
+__device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int dax, int day, int daz, float& tmx,
+                                                  float& tmy, float& tmz, float tdx, float tdy, float tdz) {
+    int b;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
+        ".reg .b32 ra;\n\t"
+        ".reg .s32 rv;\n\t"
+        "mov.b32 %0, -1;\n\t"
+        "MC_SPLIT_LOOP:\n\t"
+        "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pby|pzy, %2, %3, pna;\n\t"
+        "or.pred pz, pzx, pzy;\n\t"
+        "@pbx add.s32 %4, %4, %6;\n\t"
+        "@pby add.s32 %4, %4, %7;\n\t"
+        "@pz add.s32 %4, %4, %8;\n\t"
+        "@pbx add.s32 %5, %5, %9;\n\t"
+        "@pby add.s32 %5, %5, %10;\n\t"
+        "@pz add.s32 %5, %5, %11;\n\t"
+        "and.b32 ra, %5, %12;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "@pq bra MC_SPLIT_DONE;\n\t"
+        "ld.shared.s8 rv, [%4];\n\t"
+        "setp.ge.s32 pq, rv, 0;\n\t"
+        "@pq bra MC_SPLIT_HIT;\n\t"
+        "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %13;\n\t"
+        "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %14;\n\t"
+        "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %15;\n\t"
+        "bra MC_SPLIT_LOOP;\n\t"
+        "MC_SPLIT_HIT:\n\t"
+        "mov.b32 %0, rv;\n\t"
+        "MC_SPLIT_DONE:\n\t"
+        "}"
+        : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(addr), "+r"(cnt)
+        : "r"(dax), "r"(day), "r"(daz), "n"((1 << 7) | (1 << 21)), "n"((1 << 14) | (1 << 21)), "n"(1 | (1 << 21)),
+          "n"(kSplitGuard), "f"(tdx), "f"(tdy), "f"(tdz)
         : "memory");
     return b;
 }
@@ -669,6 +735,47 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
     int step = 0;
+    if constexpr (std::is_same<V, VoxShared>::value || std::is_same<V, VoxEither>::value) {
+        bool staged = true;
+        if constexpr (std::is_same<V, VoxEither>::value) staged = vox.smem;
+        if (!FASTG && sky_exit && staged && max_steps > 0 && wx <= 64 && wy <= 64 && wz <= 64) {
+            // A staged world and the eye inside the box: the PTX marches.
+            // They test view_distance once, at the hit: t never decreases
+            // along the ray, so a first hit closer than view_distance is the
+            // reference's hit, and a first hit at or beyond it means the
+            // reference had already ended the ray as sky (its `t >= vd`
+            // break); a ray that leaves the box or runs out of steps is sky
+            // in both.
+            int b = skip_first ? (int)AIR : (int)vox(idx);
+            // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+            const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+                      cz = (sz > 0) ? wz - 1 - vz : vz;
+            if (b < 0) {
+                const uint32_t base = (uint32_t)__cvta_generic_to_shared(vox.w);
+                if (vd_safe && max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
+                    // index and in-box counts in one register (march_packed_shared)
+                    const int packed = (idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz);
+                    b = march_packed_shared(base, packed, (dix << 18) + (1 << 12), (diy << 18) + (1 << 6),
+                                            (diz << 18) + 1, tmx, tmy, tmz, tdx, tdy, tdz);
+                } else {
+                    b = march_split_shared(base + idx, split_counts(cx, cy, cz, max_steps, wx, wy, wz), dix, diy,
+                                           diz, tmx, tmy, tmz, tdx, tdy, tdz);
+                }
+                if (b >= 0) {
+                    // the axis of the last step, chosen again from the same distances
+                    const bool bx = tmx < tmy && tmx < tmz;
+                    const bool by = !bx && tmy < tmz;
+                    t = bx ? tmx : (by ? tmy : tmz);
+                    face = bx ? 0 : (by ? 1 : 2);
+                    if (t >= vd) b = AIR;
+                }
+            }
+            h.blk = (b >= 0) ? b : AIR;
+            h.face = face;
+            h.t = t;
+            return h;
+        }
+    }
     if (!FASTG && sky_exit && vd_safe && max_steps > 0) {
         // The same march with no distance test and no branch per axis: the
         // reference's if / else-if / else choice of axis (kernels.cu:239-255)
@@ -691,22 +798,6 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             int packed = (idx << 18) | (fx << 12) | (fy << 6) | fz;
             const int px = (dix << 18) + (1 << 12), py = (diy << 18) + (1 << 6), pz = (diz << 18) + 1;
             constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
-            if constexpr (std::is_same<V, VoxShared>::value) {
-                if (b < 0) {
-                    b = (int8_t)march_packed_shared((uint32_t)__cvta_generic_to_shared(vox.w), packed, px, py, pz,
-                                                    tmx, tmy, tmz, tdx, tdy, tdz);
-                    if (b >= 0) {
-                        const bool bx = tmx < tmy && tmx < tmz;
-                        const bool by = !bx && tmy < tmz;
-                        t = bx ? tmx : (by ? tmy : tmz);
-                        face = bx ? 0 : (by ? 1 : 2);
-                    }
-                }
-                h.blk = (b >= 0) ? (int)b : AIR;
-                h.face = face;
-                h.t = t;
-                return h;
-            }
             while (b < 0) {
                 const bool bx = tmx < tmy && tmx < tmz;
                 const bool by = !bx && tmy < tmz;
@@ -2137,7 +2228,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
             if (r.bits & MC_ER_BURIED)
                 fill_env<FAM, F32>(p, e, r, cx, coop ? wt * 32 + lane : lane, coop ? nthr : 32);
             else
-                render_env<FAM, F32>(p, e, r, cx, VoxGlobal{staged ? world : gw}, rk.tile_w[g], lane,
+                render_env<FAM, F32>(p, e, r, cx, VoxEither{staged ? world : gw, staged}, rk.tile_w[g], lane,
                                      coop ? &ts->band_ctr : nullptr);
         }
         if (claimer) ts->unit[(k + 1) & 1] = claim(k + 1);
