@@ -650,6 +650,46 @@ __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int da
     return b;
 }
 
+// March from the eye's voxel (index idx, in-box steps left cx, cy, cz) through
+// a world staged at shared address `base`: the packed form where the world
+// is small and every ray leaves the box before max_steps, else the split form.
+__device__ __forceinline__ int march_staged(uint32_t base, int idx, int cx, int cy, int cz, int dix, int diy, int diz,
+                                           int wx, int wy, int wz, int max_steps, float& tmx, float& tmy, float& tmz,
+                                           float tdx, float tdy, float tdz) {
+    if (max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
+        const int packed = (idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz);
+        return march_packed_shared(base, packed, (dix << 18) + (1 << 12), (diy << 18) + (1 << 6), (diz << 18) + 1,
+                                   tmx, tmy, tmz, tdx, tdy, tdz);
+    }
+    return march_split_shared(base + idx, split_counts(cx, cy, cz, max_steps, wx, wy, wz), dix, diy, diz, tmx, tmy,
+                              tmz, tdx, tdy, tdz);
+}
+
+// Whether a march can run on the staged copy: V is a shared-memory source
+// (or one flagged as such) and the world fits the counts' 64-voxel range.
+template <class V>
+__device__ __forceinline__ bool staged_source(const V& vox, int wx, int wy, int wz) {
+    if constexpr (std::is_same<V, VoxShared>::value) {
+        return wx <= 64 && wy <= 64 && wz <= 64;
+    } else if constexpr (std::is_same<V, VoxEither>::value) {
+        return vox.smem && wx <= 64 && wy <= 64 && wz <= 64;
+    } else {
+        (void)vox; (void)wx; (void)wy; (void)wz;
+        return false;
+    }
+}
+// The shared-memory address of a staged source (0 for the others, which
+// staged_source turns away).
+template <class V>
+__device__ __forceinline__ uint32_t staged_base(const V& vox) {
+    if constexpr (std::is_same<V, VoxShared>::value || std::is_same<V, VoxEither>::value) {
+        return (uint32_t)__cvta_generic_to_shared(vox.w);
+    } else {
+        (void)vox;
+        return 0u;
+    }
+}
+
 // ray_intersects_aabb (kernels.cu:51-79) exit distance for a box [0, ws]^3
 // given the precomputed numerators (0 - eye) and (ws - eye).
 __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float lo_x, float hi_x,
@@ -992,7 +1032,8 @@ __device__ __forceinline__ uint32_t to_u8(float x) {
 // max_steps: a ray that left never re-enters, so both end as sky.
 template <bool TRIG, class V>
 __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
-                                        int wz, int max_steps, bool skip_first = false, bool sky_exit = false) {
+                                        int wz, int max_steps, bool skip_first = false, bool sky_exit = false,
+                                        int ytop = 1 << 20) {
     float ray_x, ray_y, ray_z;
     ray_dir<TRIG>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
@@ -1019,6 +1060,24 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
     int face = -1;
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
+    if (sky_exit && max_steps > 0 && staged_source(vox, wx, wy, wz)) {
+        // the PTX marches over the staged world (as in shade_ray, no view distance)
+        int b = skip_first ? (int)AIR : (int)vox(idx);
+        if (b < 0) {
+            // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+            const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+                      cz = (sz > 0) ? wz - 1 - vz : vz;
+            b = march_staged(staged_base(vox), idx, cx, cy, cz, dix, diy, diz, wx, wy, wz, max_steps, tmx, tmy, tmz,
+                             tdx, tdy, tdz);
+            if (b >= 0) {
+                const bool bx = tmx < tmy && tmx < tmz;
+                face = bx ? 0 : ((tmy < tmz) ? 1 : 2);
+            }
+        }
+        h.blk = (b >= 0) ? b : AIR;
+        h.face = face;
+        return h;
+    }
     if (sky_exit) {
         // branch-free axis choice as in shade_ray; one exit test per iteration
         int8_t b = AIR;
@@ -1485,7 +1544,8 @@ __device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const 
         return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
                                                     inside, skip_first, sky_exit, vd_safe, ytop);
     if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
-    return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
+    return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit,
+                                              ytop);
 }
 
 __device__ __forceinline__ void mbar_init_warp(uint32_t mbar_a, int lane) {
@@ -1775,7 +1835,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                         else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     } else {
                         constexpr bool TRIG = (FAM != MC_FAM_PREBASIS);
-                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
+                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit, ytop);
                         else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
                     }
                     const int so = ly * W + px;  // pixel within the staged band
