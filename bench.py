@@ -595,7 +595,7 @@ def run_reference(args):
 # The server queues up to 2 launches on the device and caps one launch at
 # 16,384 envs.
 SERVE_SEED = 5
-SERVE_LOADS = (0.2, 0.4, 0.6, 0.8, 1.0, 1.2)
+SERVE_LOADS = (0.2, 0.4, 0.6, 0.8, 0.85, 0.9, 0.95, 1.0, 1.2)
 SERVE_METRIC = "served env-steps/s at p99 step latency < 2 ms (16 jobs, mixed sizes, Poisson arrivals)"
 
 
