@@ -145,6 +145,24 @@ int mc_env_step(mc_env* env, const int8_t* buttons, const float* look, int form,
 /* The discrete form step(actions) of docs/environment.md:5-17: actions
  * uint8[B] in 0..10, look step = config.look_delta. */
 int mc_env_step_discrete(mc_env* env, const uint8_t* actions, int form, void* stream);
+/* The discrete step with host buffers: the reference's step(actions) as a
+ * caller with a host-side policy drives it (minecu/__init__.py:304-444; its
+ * rewards and dones are then copied back to the host).  actions uint8[B]
+ * are read from host memory, rewards float32[B] and dones uint8[B] written
+ * to host memory.  The copies run on the env's own upload and read-back
+ * streams and overlap the device steps of the neighbouring calls: the
+ * actions of call k+1 go up while step k runs, the results of step k come
+ * back while step k+1 runs.  Host buffers must be pinned (cudaHostAlloc or
+ * cudaHostRegister) and must stay untouched until the results of the call
+ * are known to be in host memory: after mc_env_host_join(env, s) on stream
+ * s, once s reaches that point.  The first call allocates the env's two
+ * action and two result buffers (B * 6 bytes each pair). */
+int mc_env_step_host(mc_env* env, const uint8_t* host_actions, float* host_rewards, uint8_t* host_dones, int form,
+                     void* stream);
+/* Make `stream` wait, on the device, for every copy issued by the
+ * mc_env_step_host calls so far (their host results are complete when the
+ * stream reaches this point). */
+int mc_env_host_join(mc_env* env, void* stream);
 /* MineEnv.get_obs / _render (minecu/__init__.py:446-472). */
 int mc_env_render(mc_env* env, void* stream);
 /* Regenerate every world of the env when the device byte *flag is non-zero,

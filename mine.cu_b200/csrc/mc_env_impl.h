@@ -22,6 +22,16 @@ struct RolloutGraph {
     mc_kp kp{};
 };
 
+// Double-buffered host I/O of mc_env_step_host (allocated on first use).
+struct HostIO {
+    cudaStream_t up = nullptr, down = nullptr;  // action uploads, result read-backs
+    uint8_t* d_act[2] = {nullptr, nullptr};     // B bytes each
+    uint8_t* d_res[2] = {nullptr, nullptr};     // rewards (4B bytes) then dones (B bytes)
+    cudaEvent_t act_ready[2] = {nullptr, nullptr}, act_free[2] = {nullptr, nullptr};
+    cudaEvent_t res_ready[2] = {nullptr, nullptr}, res_free[2] = {nullptr, nullptr};
+    long long calls = 0;
+};
+
 struct mc_env {
     mc_env_config cfg;
     mc_env_state st;
@@ -35,6 +45,7 @@ struct mc_env {
     uint8_t* scratch;  // plain-form decode buffers
     cudaStream_t cap_stream;
     std::vector<RolloutGraph> graphs;
+    HostIO* hio;
 };
 
 // Record a formatted message for mc_last_error() and return `code`.

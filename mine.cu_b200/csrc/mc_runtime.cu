@@ -601,8 +601,29 @@ extern "C" int mc_env_create(const mc_env_config* cfg, const mc_env_state* state
     return MC_OK;
 }
 
+static void hostio_free(mc_env* e) {
+    HostIO* h = e->hio;
+    if (!h) return;
+    for (int i = 0; i < 2; ++i) {
+        if (h->d_act[i]) cudaFree(h->d_act[i]);
+        if (h->d_res[i]) cudaFree(h->d_res[i]);
+        for (cudaEvent_t ev : {h->act_ready[i], h->act_free[i], h->res_ready[i], h->res_free[i]})
+            if (ev) cudaEventDestroy(ev);
+    }
+    if (h->up) cudaStreamDestroy(h->up);
+    if (h->down) cudaStreamDestroy(h->down);
+    delete h;
+    e->hio = nullptr;
+}
+
 extern "C" int mc_env_destroy(mc_env* e) {
     if (!e) return MC_OK;
+    if (e->hio) {
+        // copies may still be in flight into or out of the host buffers
+        if (e->hio->up) cudaStreamSynchronize(e->hio->up);
+        if (e->hio->down) cudaStreamSynchronize(e->hio->down);
+        hostio_free(e);
+    }
     drop_graphs(e);
     if (e->flags) cudaFree(e->flags);
     if (e->tmpl) cudaFree(e->tmpl);
@@ -718,6 +739,84 @@ extern "C" int mc_env_step_discrete(mc_env* e, const uint8_t* actions, int form,
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     if (e->cfg.batch_size && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
     return do_step(e, nullptr, nullptr, actions, form, (cudaStream_t)stream);
+}
+
+namespace {
+// rewards (float[B]) and dones (byte[B]) of the step just run, copied into
+// one block so that one buffer pair per step goes back to the host
+__global__ void k_results_snapshot(const float* rewards, const uint8_t* dones, long long B, uint8_t* out) {
+    float* r = reinterpret_cast<float*>(out);
+    uint8_t* d = out + 4 * B;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < B; i += (long long)gridDim.x * blockDim.x) {
+        r[i] = rewards[i];
+        d[i] = dones[i];
+    }
+}
+}  // namespace
+
+static int hostio_init(mc_env* e) {
+    if (e->hio) return MC_OK;
+    HostIO* h = new HostIO();
+    e->hio = h;
+    const size_t B = (size_t)e->cfg.batch_size;
+    cudaError_t ce = cudaStreamCreateWithFlags(&h->up, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&h->down, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && ce == cudaSuccess; ++i) {
+        ce = cudaMalloc(&h->d_act[i], B + 16);
+        if (ce == cudaSuccess) ce = cudaMalloc(&h->d_res[i], 5 * B + 16);
+        for (cudaEvent_t* ev : {&h->act_ready[i], &h->act_free[i], &h->res_ready[i], &h->res_free[i]})
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    }
+    if (ce != cudaSuccess) {
+        int rc = cuda_fail(ce, "mc_env_step_host: set-up");
+        hostio_free(e);
+        return rc;
+    }
+    return MC_OK;
+}
+
+extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* host_rewards, uint8_t* host_dones,
+                                int form, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    const long long B = e->cfg.batch_size;
+    if (B == 0) return MC_OK;
+    if (!host_actions || !host_rewards || !host_dones) return fail(MC_ERR_INVALID, "host buffers are NULL");
+    if (form != MC_FORM_PLAIN && form != MC_FORM_FUSED) return fail(MC_ERR_INVALID, "unknown form %d", form);
+    int rc = hostio_init(e);
+    if (rc) return rc;
+    HostIO* h = e->hio;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int i = (int)(h->calls & 1);
+    // upload: the step two calls back must be done reading this buffer
+    MC_CK(cudaStreamWaitEvent(h->up, h->act_free[i], 0));
+    MC_CK(cudaMemcpyAsync(h->d_act[i], host_actions, (size_t)B, cudaMemcpyHostToDevice, h->up));
+    MC_CK(cudaEventRecord(h->act_ready[i], h->up));
+    // the step on the caller's stream
+    MC_CK(cudaStreamWaitEvent(s, h->act_ready[i], 0));
+    rc = do_step(e, nullptr, nullptr, h->d_act[i], form, s);
+    if (rc) return rc;
+    MC_CK(cudaEventRecord(h->act_free[i], s));
+    // results into this call's buffer once the read-back two calls back is done with it
+    MC_CK(cudaStreamWaitEvent(s, h->res_free[i], 0));
+    const int grid = (int)std::min<long long>((B + 255) / 256, (long long)e->num_sms * 4);
+    k_results_snapshot<<<grid, 256, 0, s>>>(e->st.rewards, e->st.do_reset, B, h->d_res[i]);
+    MC_CK(cudaGetLastError());
+    MC_CK(cudaEventRecord(h->res_ready[i], s));
+    // read-back while the next step runs
+    MC_CK(cudaStreamWaitEvent(h->down, h->res_ready[i], 0));
+    MC_CK(cudaMemcpyAsync(host_rewards, h->d_res[i], (size_t)B * 4, cudaMemcpyDeviceToHost, h->down));
+    MC_CK(cudaMemcpyAsync(host_dones, h->d_res[i] + 4 * B, (size_t)B, cudaMemcpyDeviceToHost, h->down));
+    MC_CK(cudaEventRecord(h->res_free[i], h->down));
+    h->calls++;
+    return MC_OK;
+}
+
+extern "C" int mc_env_host_join(mc_env* e, void* stream) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (!e->hio || e->hio->calls == 0) return MC_OK;
+    // the read-back stream runs in call order: its last event covers every copy
+    MC_CK(cudaStreamWaitEvent((cudaStream_t)stream, e->hio->res_free[(e->hio->calls - 1) & 1], 0));
+    return MC_OK;
 }
 
 extern "C" int mc_env_regenerate_if(mc_env* e, const uint8_t* flag, void* stream) {

@@ -472,6 +472,29 @@ void env_step_discrete(std::shared_ptr<Env> e, torch::Tensor actions, int form) 
     ck(mc_env_step_discrete(e->h, ptr<uint8_t>(actions), form, cur_stream()), "step");
 }
 
+// Host tensors of mc_env_step_host: pinned CPU memory, contiguous, n entries.
+void need_pinned(const torch::Tensor& t, const char* name, std::initializer_list<at::ScalarType> dts, int64_t n) {
+    TORCH_CHECK(!t.is_cuda(), name, " must be a host (CPU) tensor");
+    bool ok = false;
+    for (auto dt : dts) ok |= t.scalar_type() == dt;
+    TORCH_CHECK(ok, name, " has dtype ", c10::toString(t.scalar_type()), ", which this call does not take");
+    TORCH_CHECK(t.is_contiguous(), name, " must be contiguous");
+    TORCH_CHECK(t.numel() == n, name, " must have ", n, " entries, got ", t.numel());
+    TORCH_CHECK(t.is_pinned(), name, " must be in pinned memory (tensor.pin_memory())");
+}
+
+void env_step_host(std::shared_ptr<Env> e, torch::Tensor actions, torch::Tensor rewards, torch::Tensor dones,
+                   int64_t batch, int form) {
+    need_pinned(actions, "actions", {at::kByte}, batch);
+    need_pinned(rewards, "rewards_out", {at::kFloat}, batch);
+    need_pinned(dones, "dones_out", {at::kBool, at::kByte}, batch);
+    ck(mc_env_step_host(e->h, static_cast<const uint8_t*>(actions.data_ptr()), rewards.data_ptr<float>(),
+                        static_cast<uint8_t*>(dones.data_ptr()), form, cur_stream()),
+       "step_host");
+}
+
+void env_host_join(std::shared_ptr<Env> e) { ck(mc_env_host_join(e->h, cur_stream()), "host_join"); }
+
 void env_render(std::shared_ptr<Env> e) { ck(mc_env_render(e->h, cur_stream()), "render"); }
 
 void env_regenerate_if(std::shared_ptr<Env> e, torch::Tensor flag) {
@@ -685,6 +708,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("env_reset", &env_reset, py::arg("env"), py::arg("mask") = py::none());
     m.def("env_step", &env_step);
     m.def("env_step_discrete", &env_step_discrete);
+    m.def("env_step_host", &env_step_host);
+    m.def("env_host_join", &env_host_join);
     m.def("env_render", &env_render);
     m.def("env_regenerate_if", &env_regenerate_if);
     m.def("env_rollout", &env_rollout, py::arg("env"), py::arg("actions"), py::arg("rewards_out") = py::none(),

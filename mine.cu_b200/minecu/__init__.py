@@ -310,6 +310,26 @@ class MineEnv:
                 _C.env_step(self._env, b, lk, form)
             return self.obs_buffer, self.rewards, self.do_reset.clone()
 
+    def step_host(self, actions: torch.Tensor, rewards_out: torch.Tensor, dones_out: torch.Tensor) -> torch.Tensor:
+        """The discrete step for a host-side policy: actions uint8 [B] read
+        from pinned host memory, rewards float32 [B] and dones bool [B]
+        written to pinned host memory.  Returns the (device) observation
+        buffer.  The copies overlap the device steps of the neighbouring
+        calls, so a call's host tensors stay in use until `join_host()` and
+        a synchronisation of the current stream (e.g.
+        torch.cuda.synchronize()): its actions must not be overwritten, nor
+        its rewards and dones read, before then."""
+        form = FORMS[self.form]
+        with torch.cuda.device(self.device):
+            _C.env_step_host(self._env, actions, rewards_out, dones_out, self.batch_size, form)
+        return self.obs_buffer
+
+    def join_host(self) -> None:
+        """Make the current stream wait for the host copies of every
+        step_host call so far."""
+        with torch.cuda.device(self.device):
+            _C.env_host_join(self._env)
+
     def rollout(self, actions: torch.Tensor, rewards_out: Optional[torch.Tensor] = None,
                 dones_out: Optional[torch.Tensor] = None) -> None:
         """K fused steps of discrete actions [K, B] (uint8, on the device),

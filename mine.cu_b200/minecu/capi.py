@@ -108,6 +108,8 @@ _PROTOS = {
     "mc_env_reset": (I, [P, P, P]),
     "mc_env_step": (I, [P, P, P, ctypes.c_int, P]),
     "mc_env_step_discrete": (I, [P, P, ctypes.c_int, P]),
+    "mc_env_step_host": (I, [P, P, P, P, ctypes.c_int, P]),
+    "mc_env_host_join": (I, [P, P]),
     "mc_env_render": (I, [P, P]),
     "mc_env_regenerate_if": (I, [P, P, P]),
     "mc_env_rollout": (I, [P, P, I, P, P, P]),

@@ -1,0 +1,77 @@
+"""MineEnv.step_host (mc_env_step_host): the discrete step with host buffers,
+whose uploads and read-backs overlap the neighbouring steps.
+
+Two envs built alike take the same actions: one through step(actions) with
+device tensors, the other through step_host with pinned host tensors.  After
+join_host and a synchronisation, every step's rewards and dones in host
+memory, and the final state of the two envs, must be identical (floats
+compared as int32 bit patterns; tolerance none).  Short episodes and half of
+the actions forced to "break" make rewards, dones and world regeneration
+happen inside the window.
+"""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("voxels", "positions", "velocities", "yaws", "pitches", "on_ground", "step_count", "do_reset", "cameras",
+        "rewards", "obs_buffer")
+
+
+def _pair(cuda, form, **kw):
+    from minecu import MineEnv
+    envs = [MineEnv(device=cuda, **kw) for _ in range(2)]
+    for e in envs:
+        e.form = form
+        e.reset()
+    return envs
+
+
+@pytest.mark.parametrize("form", ["fused", "plain"])
+@pytest.mark.parametrize("shape", [dict(batch_size=300, world_size=16, render_width=32, render_height=32,
+                                        episode_length=7, obs_dtype="uint8"),
+                                   dict(batch_size=77, world_size=32, render_width=24, render_height=16,
+                                        episode_length=5, obs_dtype="float32")])
+def test_step_host_matches_step(cuda, form, shape):
+    import torch
+    from minecu import _C
+    ref, host = _pair(cuda, form, **shape)
+    B, K = shape["batch_size"], 23
+    acts = torch.empty((K, B), dtype=torch.uint8, device=cuda)
+    _C.philox_actions(acts, 0, 0, 11, True)
+    h_acts = acts.cpu().pin_memory()
+    h_rew = torch.zeros((K, B), dtype=torch.float32).pin_memory()
+    h_done = torch.zeros((K, B), dtype=torch.bool).pin_memory()
+    want_rew, want_done = [], []
+    for s in range(K):
+        _, r, d = ref.step(acts[s])
+        want_rew.append(r.clone())
+        want_done.append(d.clone())
+        host.step_host(h_acts[s], h_rew[s], h_done[s])
+    host.join_host()
+    torch.cuda.synchronize()
+    want_rew = torch.stack(want_rew).cpu()
+    want_done = torch.stack(want_done).cpu()
+    assert torch.equal(h_rew.view(torch.int32), want_rew.view(torch.int32))
+    assert torch.equal(h_done, want_done.to(torch.bool))
+    assert bool(want_done.any()), "the window should end episodes"
+    assert bool((want_rew != 0).any()), "the window should earn rewards"
+    for k in KEYS:
+        a, b = getattr(ref, k), getattr(host, k)
+        if a.dtype == torch.float32:
+            a, b = a.view(torch.int32), b.view(torch.int32)
+        assert torch.equal(a, b), k
+
+
+def test_step_host_rejects_device_and_pageable_buffers(cuda):
+    import torch
+    from minecu import MineEnv
+    env = MineEnv(batch_size=8, world_size=8, render_width=8, render_height=8, ground_height=4, device=cuda)
+    env.reset()
+    rew = torch.zeros(8, dtype=torch.float32).pin_memory()
+    done = torch.zeros(8, dtype=torch.bool).pin_memory()
+    with pytest.raises(RuntimeError, match="pinned"):
+        env.step_host(torch.zeros(8, dtype=torch.uint8), rew, done)
+    with pytest.raises(RuntimeError, match="host"):
+        env.step_host(torch.zeros(8, dtype=torch.uint8, device=cuda), rew, done)
+    with pytest.raises(RuntimeError, match="entries"):
+        env.step_host(torch.zeros(9, dtype=torch.uint8).pin_memory(), rew, done)
