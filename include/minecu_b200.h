@@ -218,6 +218,16 @@ int64_t mc_ragged_smem_bytes(const mc_ragged* r);
 int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* look, void* stream);
 /* One step of every group: discrete actions uint8[total]. */
 int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, void* stream);
+/* The discrete step of every group with host buffers, as mc_env_step_host:
+ * actions uint8[total] from pinned host memory, every env's reward
+ * float32[total] and done uint8[total] (concatenated in group order) to
+ * pinned host memory, the copies overlapping the neighbouring steps; the
+ * launch writes the results straight into the read-back buffer.  Results
+ * are in host memory once a stream given to mc_ragged_host_join reaches
+ * that point. */
+int mc_ragged_step_host(mc_ragged* r, const uint8_t* host_actions, float* host_rewards, uint8_t* host_dones,
+                        void* stream);
+int mc_ragged_host_join(mc_ragged* r, void* stream);
 /* K steps of actions uint8[K,total] in one CUDA graph (cached per actions, K and config). */
 int mc_ragged_rollout(mc_ragged* r, const uint8_t* actions, int32_t K, void* stream);
 int mc_ragged_rollout_prepare(mc_ragged* r, const uint8_t* actions, int32_t K);

@@ -601,8 +601,8 @@ extern "C" int mc_env_create(const mc_env_config* cfg, const mc_env_state* state
     return MC_OK;
 }
 
-static void hostio_free(mc_env* e) {
-    HostIO* h = e->hio;
+static void hostio_free(HostIO** ph) {
+    HostIO* h = *ph;
     if (!h) return;
     for (int i = 0; i < 2; ++i) {
         if (h->d_act[i]) cudaFree(h->d_act[i]);
@@ -613,17 +613,20 @@ static void hostio_free(mc_env* e) {
     if (h->up) cudaStreamDestroy(h->up);
     if (h->down) cudaStreamDestroy(h->down);
     delete h;
-    e->hio = nullptr;
+    *ph = nullptr;
+}
+
+// Wait for the copies in flight into or out of the caller's host buffers, then free.
+static void hostio_close(HostIO** ph) {
+    if (!*ph) return;
+    if ((*ph)->up) cudaStreamSynchronize((*ph)->up);
+    if ((*ph)->down) cudaStreamSynchronize((*ph)->down);
+    hostio_free(ph);
 }
 
 extern "C" int mc_env_destroy(mc_env* e) {
     if (!e) return MC_OK;
-    if (e->hio) {
-        // copies may still be in flight into or out of the host buffers
-        if (e->hio->up) cudaStreamSynchronize(e->hio->up);
-        if (e->hio->down) cudaStreamSynchronize(e->hio->down);
-        hostio_free(e);
-    }
+    hostio_close(&e->hio);
     drop_graphs(e);
     if (e->flags) cudaFree(e->flags);
     if (e->tmpl) cudaFree(e->tmpl);
@@ -754,11 +757,11 @@ __global__ void k_results_snapshot(const float* rewards, const uint8_t* dones, l
 }
 }  // namespace
 
-static int hostio_init(mc_env* e) {
-    if (e->hio) return MC_OK;
+static int hostio_init(HostIO** ph, long long batch) {
+    if (*ph) return MC_OK;
     HostIO* h = new HostIO();
-    e->hio = h;
-    const size_t B = (size_t)e->cfg.batch_size;
+    *ph = h;
+    const size_t B = (size_t)batch;
     cudaError_t ce = cudaStreamCreateWithFlags(&h->up, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&h->down, cudaStreamNonBlocking);
     for (int i = 0; i < 2 && ce == cudaSuccess; ++i) {
@@ -768,10 +771,39 @@ static int hostio_init(mc_env* e) {
             if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     }
     if (ce != cudaSuccess) {
-        int rc = cuda_fail(ce, "mc_env_step_host: set-up");
-        hostio_free(e);
+        int rc = cuda_fail(ce, "host-buffer step: set-up");
+        hostio_free(ph);
         return rc;
     }
+    return MC_OK;
+}
+
+// Upload of call k's actions into action buffer i (= k mod 2) once the step
+// two calls back is done reading it; stream s waits for the upload.
+static int hostio_upload(HostIO* h, int i, const uint8_t* host_actions, long long B, cudaStream_t s) {
+    MC_CK(cudaStreamWaitEvent(h->up, h->act_free[i], 0));
+    MC_CK(cudaMemcpyAsync(h->d_act[i], host_actions, (size_t)B, cudaMemcpyHostToDevice, h->up));
+    MC_CK(cudaEventRecord(h->act_ready[i], h->up));
+    MC_CK(cudaStreamWaitEvent(s, h->act_ready[i], 0));
+    return MC_OK;
+}
+
+// Read-back of result buffer i (rewards then dones, written on stream s)
+// while the next step runs; ends the call.
+static int hostio_readback(HostIO* h, int i, float* host_rewards, uint8_t* host_dones, long long B, cudaStream_t s) {
+    MC_CK(cudaEventRecord(h->res_ready[i], s));
+    MC_CK(cudaStreamWaitEvent(h->down, h->res_ready[i], 0));
+    MC_CK(cudaMemcpyAsync(host_rewards, h->d_res[i], (size_t)B * 4, cudaMemcpyDeviceToHost, h->down));
+    MC_CK(cudaMemcpyAsync(host_dones, h->d_res[i] + 4 * B, (size_t)B, cudaMemcpyDeviceToHost, h->down));
+    MC_CK(cudaEventRecord(h->res_free[i], h->down));
+    h->calls++;
+    return MC_OK;
+}
+
+static int hostio_join(const HostIO* h, cudaStream_t s) {
+    if (!h || h->calls == 0) return MC_OK;
+    // the read-back stream runs in call order: its last event covers every copy
+    MC_CK(cudaStreamWaitEvent(s, h->res_free[(h->calls - 1) & 1], 0));
     return MC_OK;
 }
 
@@ -782,17 +814,13 @@ extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* h
     if (B == 0) return MC_OK;
     if (!host_actions || !host_rewards || !host_dones) return fail(MC_ERR_INVALID, "host buffers are NULL");
     if (form != MC_FORM_PLAIN && form != MC_FORM_FUSED) return fail(MC_ERR_INVALID, "unknown form %d", form);
-    int rc = hostio_init(e);
+    int rc = hostio_init(&e->hio, B);
     if (rc) return rc;
     HostIO* h = e->hio;
     cudaStream_t s = (cudaStream_t)stream;
     const int i = (int)(h->calls & 1);
-    // upload: the step two calls back must be done reading this buffer
-    MC_CK(cudaStreamWaitEvent(h->up, h->act_free[i], 0));
-    MC_CK(cudaMemcpyAsync(h->d_act[i], host_actions, (size_t)B, cudaMemcpyHostToDevice, h->up));
-    MC_CK(cudaEventRecord(h->act_ready[i], h->up));
-    // the step on the caller's stream
-    MC_CK(cudaStreamWaitEvent(s, h->act_ready[i], 0));
+    rc = hostio_upload(h, i, host_actions, B, s);
+    if (rc) return rc;
     rc = do_step(e, nullptr, nullptr, h->d_act[i], form, s);
     if (rc) return rc;
     MC_CK(cudaEventRecord(h->act_free[i], s));
@@ -801,22 +829,12 @@ extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* h
     const int grid = (int)std::min<long long>((B + 255) / 256, (long long)e->num_sms * 4);
     k_results_snapshot<<<grid, 256, 0, s>>>(e->st.rewards, e->st.do_reset, B, h->d_res[i]);
     MC_CK(cudaGetLastError());
-    MC_CK(cudaEventRecord(h->res_ready[i], s));
-    // read-back while the next step runs
-    MC_CK(cudaStreamWaitEvent(h->down, h->res_ready[i], 0));
-    MC_CK(cudaMemcpyAsync(host_rewards, h->d_res[i], (size_t)B * 4, cudaMemcpyDeviceToHost, h->down));
-    MC_CK(cudaMemcpyAsync(host_dones, h->d_res[i] + 4 * B, (size_t)B, cudaMemcpyDeviceToHost, h->down));
-    MC_CK(cudaEventRecord(h->res_free[i], h->down));
-    h->calls++;
-    return MC_OK;
+    return hostio_readback(h, i, host_rewards, host_dones, B, s);
 }
 
 extern "C" int mc_env_host_join(mc_env* e, void* stream) {
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
-    if (!e->hio || e->hio->calls == 0) return MC_OK;
-    // the read-back stream runs in call order: its last event covers every copy
-    MC_CK(cudaStreamWaitEvent((cudaStream_t)stream, e->hio->res_free[(e->hio->calls - 1) & 1], 0));
-    return MC_OK;
+    return hostio_join(e->hio, (cudaStream_t)stream);
 }
 
 extern "C" int mc_env_regenerate_if(mc_env* e, const uint8_t* flag, void* stream) {
@@ -989,6 +1007,7 @@ struct mc_ragged {
     long long version = 1;
     cudaStream_t cap_stream = nullptr;
     std::vector<RaggedGraph> graphs;
+    HostIO* hio = nullptr;  // mc_ragged_step_host buffers
 };
 
 static long long ragged_wxyz(const mc_env* e) {
@@ -1100,6 +1119,7 @@ extern "C" int mc_ragged_create(mc_env* const* groups, int32_t ngroups, mc_ragge
 
 extern "C" int mc_ragged_destroy(mc_ragged* r) {
     if (!r) return MC_OK;
+    hostio_close(&r->hio);
     ragged_drop_graphs(r);
     if (r->flags) cudaFree(r->flags);
     if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
@@ -1138,11 +1158,14 @@ extern "C" int64_t mc_ragged_smem_bytes(const mc_ragged* r) {
 }
 
 static int ragged_do_step(mc_ragged* r, const int8_t* buttons, const float* look, const uint8_t* actions,
-                          cudaStream_t s, bool capturing) {
+                          cudaStream_t s, bool capturing, float* rewards_cat = nullptr,
+                          uint8_t* dones_cat = nullptr) {
     int rc = ragged_sync_groups(r, capturing);
     if (rc) return rc;
     mc_ragged_kp rk;
     ragged_layout(r, &r->cfg, &rk);
+    rk.rewards_cat = rewards_cat;  // every env's reward and done also at its index in the batch
+    rk.dones_cat = dones_cat;
     rk.actions = actions;
     rk.buttons = buttons;
     rk.look = look;
@@ -1169,6 +1192,34 @@ extern "C" int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, voi
     if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
     if (mc_ragged_total_envs(r) > 0 && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
     return ragged_do_step(r, nullptr, nullptr, actions, (cudaStream_t)stream, false);
+}
+
+extern "C" int mc_ragged_step_host(mc_ragged* r, const uint8_t* host_actions, float* host_rewards,
+                                   uint8_t* host_dones, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    const long long B = mc_ragged_total_envs(r);
+    if (B == 0) return MC_OK;
+    if (!host_actions || !host_rewards || !host_dones) return fail(MC_ERR_INVALID, "host buffers are NULL");
+    int rc = hostio_init(&r->hio, B);
+    if (rc) return rc;
+    HostIO* h = r->hio;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int i = (int)(h->calls & 1);
+    rc = hostio_upload(h, i, host_actions, B, s);
+    if (rc) return rc;
+    // the team kernel writes the results straight into this call's buffer,
+    // once the read-back two calls back is done with it
+    MC_CK(cudaStreamWaitEvent(s, h->res_free[i], 0));
+    rc = ragged_do_step(r, nullptr, nullptr, h->d_act[i], s, false, reinterpret_cast<float*>(h->d_res[i]),
+                        h->d_res[i] + 4 * B);
+    if (rc) return rc;
+    MC_CK(cudaEventRecord(h->act_free[i], s));
+    return hostio_readback(h, i, host_rewards, host_dones, B, s);
+}
+
+extern "C" int mc_ragged_host_join(mc_ragged* r, void* stream) {
+    if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
+    return hostio_join(r->hio, (cudaStream_t)stream);
 }
 
 static int ragged_graph(mc_ragged* r, const uint8_t* actions, int32_t K, RaggedGraph** out) {

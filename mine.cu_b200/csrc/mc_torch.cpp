@@ -617,6 +617,18 @@ void ragged_step_discrete(std::shared_ptr<Ragged> r, torch::Tensor actions) {
     ck(mc_ragged_step_discrete(r->h, ptr<uint8_t>(actions), cur_stream()), "ragged_step");
 }
 
+void ragged_step_host(std::shared_ptr<Ragged> r, torch::Tensor actions, torch::Tensor rewards, torch::Tensor dones) {
+    const int64_t n = mc_ragged_total_envs(r->h);
+    need_pinned(actions, "actions", {at::kByte}, n);
+    need_pinned(rewards, "rewards_out", {at::kFloat}, n);
+    need_pinned(dones, "dones_out", {at::kBool, at::kByte}, n);
+    ck(mc_ragged_step_host(r->h, static_cast<const uint8_t*>(actions.data_ptr()), rewards.data_ptr<float>(),
+                           static_cast<uint8_t*>(dones.data_ptr()), cur_stream()),
+       "ragged_step_host");
+}
+
+void ragged_host_join(std::shared_ptr<Ragged> r) { ck(mc_ragged_host_join(r->h, cur_stream()), "ragged_host_join"); }
+
 void ragged_rollout(std::shared_ptr<Ragged> r, torch::Tensor actions, bool prepare_only) {
     need(actions, "actions", at::kByte);
     TORCH_CHECK(actions.dim() == 2 && actions.size(1) == mc_ragged_total_envs(r->h), "actions must be [K, total]");
@@ -722,6 +734,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     py::class_<Ragged, std::shared_ptr<Ragged>>(m, "Ragged");
     m.def("ragged_create", &ragged_create);
     m.def("ragged_set_config", &ragged_set_config);
+    m.def("ragged_step_host", &ragged_step_host);
+    m.def("ragged_host_join", &ragged_host_join);
     m.def("ragged_get_config", &ragged_get_config);
     m.def("ragged_total_envs", &ragged_total_envs);
     m.def("ragged_step", &ragged_step);

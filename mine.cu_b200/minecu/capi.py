@@ -126,6 +126,8 @@ _PROTOS = {
     "mc_ragged_smem_bytes": (ctypes.c_int64, [P]),
     "mc_ragged_step": (I, [P, P, P, P]),
     "mc_ragged_step_discrete": (I, [P, P, P]),
+    "mc_ragged_step_host": (I, [P, P, P, P, P]),
+    "mc_ragged_host_join": (I, [P, P]),
     "mc_ragged_rollout": (I, [P, P, I, P]),
     "mc_ragged_rollout_prepare": (I, [P, P, I]),
     "mc_ragged_check_error": (I, [P, P]),

@@ -82,6 +82,24 @@ class RaggedBatch:
                 _C.ragged_step(self._r, b, lk)
         return [(e.obs_buffer, e.rewards, e.do_reset.clone()) for e in self.envs]
 
+    def step_host(self, actions: torch.Tensor, rewards_out: torch.Tensor, dones_out: torch.Tensor
+                  ) -> List[torch.Tensor]:
+        """One discrete step of every group with host buffers, as
+        MineEnv.step_host: actions uint8 [total] from pinned host memory,
+        rewards float32 [total] and dones bool [total] (group order) to
+        pinned host memory, valid after `join_host()` and a synchronisation
+        of the current stream.  Returns each group's (device) observation
+        buffer."""
+        with torch.cuda.device(self.device):
+            _C.ragged_step_host(self._r, actions, rewards_out, dones_out)
+        return [e.obs_buffer for e in self.envs]
+
+    def join_host(self) -> None:
+        """Make the current stream wait for the host copies of every
+        step_host call so far."""
+        with torch.cuda.device(self.device):
+            _C.ragged_host_join(self._r)
+
     def rollout(self, actions: torch.Tensor) -> None:
         """K steps of discrete actions uint8 [K, total] captured once in a
         CUDA graph and replayed."""

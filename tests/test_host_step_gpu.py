@@ -75,3 +75,46 @@ def test_step_host_rejects_device_and_pageable_buffers(cuda):
         env.step_host(torch.zeros(8, dtype=torch.uint8, device=cuda), rew, done)
     with pytest.raises(RuntimeError, match="entries"):
         env.step_host(torch.zeros(9, dtype=torch.uint8).pin_memory(), rew, done)
+
+
+def test_ragged_step_host_matches_step(cuda):
+    """RaggedBatch.step_host against RaggedBatch.step on a twin batch of four
+    groups (different worlds, resolutions and episode lengths)."""
+    import torch
+    from minecu import MineEnv, _C
+    from minecu.ragged import RaggedBatch
+    groups = [(37, 8, 16, 4, None), (50, 16, 32, 8, 9), (23, 24, 24, 8, None), (19, 32, 64, 8, 6)]
+
+    def make():
+        envs = [MineEnv(batch_size=b, world_size=w, render_width=r, render_height=r, ground_height=gh,
+                        episode_length=el, obs_dtype="uint8", device=cuda) for b, w, r, gh, el in groups]
+        batch = RaggedBatch(envs)
+        batch.reset()
+        return batch
+
+    ref, host = make(), make()
+    total, K = sum(g[0] for g in groups), 19
+    acts = torch.empty((K, total), dtype=torch.uint8, device=cuda)
+    _C.philox_actions(acts, 0, 0, 5, True)
+    h_acts = acts.cpu().pin_memory()
+    h_rew = torch.zeros((K, total), dtype=torch.float32).pin_memory()
+    h_done = torch.zeros((K, total), dtype=torch.bool).pin_memory()
+    want_rew, want_done = [], []
+    for s in range(K):
+        res = ref.step(acts[s])
+        want_rew.append(torch.cat([r.clone() for _, r, _ in res]))
+        want_done.append(torch.cat([d.clone().to(torch.bool) for _, _, d in res]))
+        host.step_host(h_acts[s], h_rew[s], h_done[s])
+    host.join_host()
+    torch.cuda.synchronize()
+    want_rew = torch.stack(want_rew).cpu()
+    want_done = torch.stack(want_done).cpu()
+    assert torch.equal(h_rew.view(torch.int32), want_rew.view(torch.int32))
+    assert torch.equal(h_done, want_done)
+    assert bool(want_done.any()) and bool((want_rew != 0).any())
+    for ga, gb in zip(ref.envs, host.envs):
+        for k in KEYS:
+            a, b = getattr(ga, k), getattr(gb, k)
+            if a.dtype == torch.float32:
+                a, b = a.view(torch.int32), b.view(torch.int32)
+            assert torch.equal(a, b), k
