@@ -549,7 +549,11 @@ struct Hit {
 // and distance updates directly (no selects), and the distance update comes
 // after the voxel test, so at a hit tm still holds the entry distances the
 // choice was made from: the caller recovers the axis and the distance t
-// from them once per ray instead of carrying them through the loop.
+// from them once per ray instead of carrying them through the loop.  The
+// voxel is loaded before the exit test, so that one test covers both exits;
+// the load of the step that leaves the box reads up to wx*wz bytes before or
+// after the staged world, which the shared-memory layouts keep allocated
+// (the value read there is not used).
 // Returns the block hit (>= 0), or -1 when the ray left the box.
 __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, int px, int py, int pz, float& tmx,
                                                    float& tmy, float& tmz, float tdx, float tdy, float tdz) {
@@ -560,7 +564,6 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
         ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
         ".reg .b32 ra;\n\t"
         ".reg .s32 rv;\n\t"
-        "mov.b32 %0, -1;\n\t"
         "MC_MARCH_LOOP:\n\t"
         "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
         "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
@@ -569,24 +572,26 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
         "@pbx add.s32 %4, %4, %5;\n\t"
         "@pby add.s32 %4, %4, %6;\n\t"
         "@pz add.s32 %4, %4, %7;\n\t"
-        "and.b32 ra, %4, %8;\n\t"
-        "setp.ne.b32 pq, ra, 0;\n\t"
-        "@pq bra MC_MARCH_DONE;\n\t"
         "shr.s32 ra, %4, 18;\n\t"
         "add.s32 ra, ra, %9;\n\t"
         "ld.shared.s8 rv, [ra];\n\t"
-        "setp.ge.s32 pq, rv, 0;\n\t"
-        "@pq bra MC_MARCH_HIT;\n\t"
+        // one test for both exits: a guard bit of the counts, or the sign
+        // bit clear in the voxel (a block); c & (a | ~b) = lut 0xA2
+        "lop3.b32 ra, %4, rv, %8, 0xA2;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "@pq bra MC_MARCH_DONE;\n\t"
         "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %10;\n\t"
         "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %11;\n\t"
         "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %12;\n\t"
         "bra MC_MARCH_LOOP;\n\t"
-        "MC_MARCH_HIT:\n\t"
-        "mov.b32 %0, rv;\n\t"
         "MC_MARCH_DONE:\n\t"
+        "and.b32 ra, %4, %13;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "selp.b32 %0, -1, rv, pq;\n\t"
         "}"
         : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(packed)
-        : "r"(px), "r"(py), "r"(pz), "n"(kGuard), "r"(world), "f"(tdx), "f"(tdy), "f"(tdz)
+        : "r"(px), "r"(py), "r"(pz), "n"(kGuard | (int)0x80000000u), "r"(world), "f"(tdx), "f"(tdy), "f"(tdz),
+          "n"(kGuard)
         : "memory");
     return b;
 }
@@ -617,7 +622,6 @@ __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int da
         ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
         ".reg .b32 ra;\n\t"
         ".reg .s32 rv;\n\t"
-        "mov.b32 %0, -1;\n\t"
         "MC_SPLIT_LOOP:\n\t"
         "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
         "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
@@ -629,23 +633,23 @@ __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int da
         "@pbx add.s32 %5, %5, %9;\n\t"
         "@pby add.s32 %5, %5, %10;\n\t"
         "@pz add.s32 %5, %5, %11;\n\t"
-        "and.b32 ra, %5, %12;\n\t"
+        "ld.shared.s8 rv, [%4];\n\t"
+        // one test for both exits (as in march_packed_shared)
+        "lop3.b32 ra, %5, rv, %12, 0xA2;\n\t"
         "setp.ne.b32 pq, ra, 0;\n\t"
         "@pq bra MC_SPLIT_DONE;\n\t"
-        "ld.shared.s8 rv, [%4];\n\t"
-        "setp.ge.s32 pq, rv, 0;\n\t"
-        "@pq bra MC_SPLIT_HIT;\n\t"
         "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %13;\n\t"
         "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %14;\n\t"
         "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %15;\n\t"
         "bra MC_SPLIT_LOOP;\n\t"
-        "MC_SPLIT_HIT:\n\t"
-        "mov.b32 %0, rv;\n\t"
         "MC_SPLIT_DONE:\n\t"
+        "and.b32 ra, %5, %16;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "selp.b32 %0, -1, rv, pq;\n\t"
         "}"
         : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(addr), "+r"(cnt)
         : "r"(dax), "r"(day), "r"(daz), "n"((1 << 7) | (1 << 21)), "n"((1 << 14) | (1 << 21)), "n"(1 | (1 << 21)),
-          "n"(kSplitGuard), "f"(tdx), "f"(tdy), "f"(tdz)
+          "n"(kSplitGuard | (int)0x80000000u), "f"(tdx), "f"(tdy), "f"(tdz), "n"(kSplitGuard)
         : "memory");
     return b;
 }
@@ -1406,11 +1410,13 @@ struct FusedLayout {
     int world_bytes;   // world bytes per warp (0 when not staged)
     int warp_bytes;    // total per warp (16-aligned)
     int head_bytes;    // tables (16-aligned)
+    int pad_bytes;     // allocated after the last warp's world
 };
 
 __host__ __device__ inline int mc_align16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int obs_f32, int stage, int tile_w) {
+__host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int wxz, int obs_f32, int stage,
+                                                   int tile_w) {
     FusedLayout L;
     L.W = W;
     L.H = H;
@@ -1420,6 +1426,11 @@ __host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int 
     L.world_bytes = stage ? mc_align16(wxyz) : 0;
     L.warp_bytes = 16 + L.stage_bytes + L.world_bytes;  // 16: mbarrier
     L.head_bytes = mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
+    // the march reads up to wx*wz bytes on either side of a staged world:
+    // keep that much allocated before the first world and after the last
+    L.pad_bytes = stage ? mc_align16(wxz) : 0;
+    const int before = L.head_bytes + 16 + L.stage_bytes;
+    if (before < L.pad_bytes) L.head_bytes += mc_align16(L.pad_bytes - before);
     return L;
 }
 
@@ -1606,7 +1617,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
     const int HW = W * H;
     const int wxz = p.wx * p.wz;
     const int wxyz = wxz * p.wy;
-    FusedLayout L = fused_layout(W, H, wxyz, F32, STAGE, tile_w);
+    FusedLayout L = fused_layout(W, H, wxyz, p.wx * p.wz, F32, STAGE, tile_w);
 
     // --- tables -------------------------------------------------------------
     float* s_u = reinterpret_cast<float*>(smem);
@@ -2353,8 +2364,8 @@ static int step_plain(const mc_kp* p, cudaStream_t s) {
 
 static size_t fused_smem(const mc_kp* p, const mc_fused_cfg* cfg) {
     int wxyz = p->wx * p->wy * p->wz;
-    FusedLayout L = fused_layout(p->W, p->H, wxyz, p->obs_f32, cfg->stage, cfg->tile_w);
-    return (size_t)L.head_bytes + (size_t)cfg->warps_per_cta * L.warp_bytes;
+    FusedLayout L = fused_layout(p->W, p->H, wxyz, p->wx * p->wz, p->obs_f32, cfg->stage, cfg->tile_w);
+    return (size_t)L.head_bytes + (size_t)cfg->warps_per_cta * L.warp_bytes + (size_t)L.pad_bytes;
 }
 
 template <int FAM, bool F32, bool STAGE>
@@ -2385,7 +2396,7 @@ static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, 
 template <int FAM, bool F32>
 static int launch_team_t(const mc_ragged_kp* rk, int warps_per_cta, int ctas_per_sm, int num_sms, cudaStream_t s) {
     auto kern = k_step_team<FAM, F32>;
-    size_t smem = (size_t)rk->warps_off + (size_t)warps_per_cta * rk->warp_bytes;
+    size_t smem = (size_t)rk->warps_off + (size_t)warps_per_cta * rk->warp_bytes + (size_t)rk->tail_bytes;
     static size_t attr_set = 0;
     if (smem > 48 * 1024 && smem > attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

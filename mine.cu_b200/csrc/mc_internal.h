@@ -120,6 +120,7 @@ struct mc_ragged_kp {
     int team_bytes;                 // MC_TEAM_HEAD_BYTES + the team's world buffer
     int slot_bytes;                 // world slot of one warp of a per-warp staged group
     int warp_bytes;                 // 16 (mbarrier) + one band of observation bytes
+    int tail_bytes;                 // allocated after the warps: the march may read one world layer past the last world
 };
 
 // One numerics back end (ref_fast or ieee).

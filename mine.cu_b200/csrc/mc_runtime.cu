@@ -420,7 +420,7 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
     rk->sched_dynamic = 1;
     const int bpp = 3 * (kps[0]->obs_f32 ? 4 : 1);
     long long start = 0;
-    int uv = 0, band = 16, coop_world = 0, slot = 0;
+    int uv = 0, band = 16, coop_world = 0, slot = 0, pad = 0;
     for (int g = 0; g < G; ++g) {
         const mc_kp& k = *kps[g];
         const long long wxyz = (long long)k.wx * k.wy * k.wz;
@@ -434,6 +434,7 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
         if (coop[g]) rk->coop_mask |= 1 << g;
         if (stage[g]) {
             rk->stage_mask |= 1 << g;
+            pad = std::max(pad, align16i((long long)k.wx * k.wz));
             if (coop[g])
                 coop_world = std::max(coop_world, align16i(wxyz));
             else
@@ -459,13 +460,19 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
     rk->slot_bytes = slot;
     rk->tables_off = MC_COLOUR_TABLE_BYTES;
     rk->teams_off = rk->tables_off + align16i((long long)uv * 4);
+    // the march reads up to one world layer (wx*wz bytes) on either side of a
+    // staged world: worlds that follow one another are farther apart than
+    // that, so only the first needs bytes before it and the last bytes after
+    if (rk->teams_off + MC_TEAM_HEAD_BYTES < pad) rk->teams_off += align16i(pad - rk->teams_off - MC_TEAM_HEAD_BYTES);
     rk->team_bytes = MC_TEAM_HEAD_BYTES + std::max(coop_world, team_warps * slot);
     rk->warps_off = rk->teams_off + (warps_per_cta / team_warps) * rk->team_bytes;
     rk->warp_bytes = 16 + band;
+    const int after = warps_per_cta * rk->warp_bytes;
+    rk->tail_bytes = after < pad ? pad - after : 0;
 }
 
 long long team_smem(const mc_ragged_kp& rk, int warps_per_cta) {
-    return (long long)rk.warps_off + (long long)warps_per_cta * rk.warp_bytes;
+    return (long long)rk.warps_off + (long long)warps_per_cta * rk.warp_bytes + rk.tail_bytes;
 }
 
 int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* tile_w, const int* coop,
