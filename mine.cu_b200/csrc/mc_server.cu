@@ -19,7 +19,9 @@
 // completer its event) instead of blocking, which keeps thread wake-ups out
 // of the request latency at the cost of two busy host cores under load.
 // Up to max_inflight launches are queued on the device at once, so the host
-// work of the next launch overlaps the current one.  A job's requests run in
+// work of the next launch overlaps the current one; the actions upload and
+// the results read-back run on their own streams, so they overlap the
+// neighbouring launches' kernels instead of queueing between them.  A job's requests run in
 // submission order (one stream).  With batching = 0 the launcher takes one
 // request at a time (oldest first) and steps with the plain form: the
 // one-job-at-a-time loop the batched server is compared with.
@@ -81,7 +83,9 @@ struct Job {
 };
 
 struct Slot {
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr;     // recorded after the read-back: the launch is complete
+    cudaEvent_t ev_up = nullptr;  // actions uploaded
+    cudaEvent_t ev_k = nullptr;   // device work of the launch done
     uint8_t* h_act = nullptr;  // pinned
     uint8_t* d_act = nullptr;
     uint8_t* h_res = nullptr;  // pinned: rewards (cap floats), then dones (cap bytes)
@@ -183,6 +187,7 @@ struct mc_server {
     bool stop = false, launcher_done = false;
     std::thread launcher, completer;
     cudaStream_t stream = nullptr, admit_stream = nullptr;
+    cudaStream_t up = nullptr, down = nullptr;  // actions uploads, results read-backs
     int32_t* flags = nullptr;  // work counter of the team launches
     Slot slots[kMaxSlots];
     int nslots = 0;
@@ -263,7 +268,9 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
             sl.offs[i] = off;
             off += r->job->cfg.batch_size;
         }
-        cudaError_t ce = cudaMemcpyAsync(sl.d_act, sl.h_act, (size_t)off, cudaMemcpyHostToDevice, st);
+        cudaError_t ce = cudaMemcpyAsync(sl.d_act, sl.h_act, (size_t)off, cudaMemcpyHostToDevice, s->up);
+        if (ce == cudaSuccess) ce = cudaEventRecord(sl.ev_up, s->up);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, sl.ev_up, 0);
         if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: actions upload");
         // rewards then dones, contiguous: one read-back
         sl.total = off;
@@ -309,10 +316,19 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
                 ce = cudaMemcpyAsync(d_done, r->job->st.do_reset, B, cudaMemcpyDeviceToDevice, st);
             if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: result gather");
         }
-        ce = cudaMemcpyAsync(sl.h_res, sl.d_res, (size_t)off * 5, cudaMemcpyDeviceToHost, st);
-        if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: results read-back");
     }
     return rc;
+}
+
+// After the device work of a launch: its results read-back on the read-back
+// stream, then the event the completer waits for.
+int finish_batch(mc_server* s, Slot& sl, bool readback) {
+    cudaError_t ce = cudaEventRecord(sl.ev_k, s->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s->down, sl.ev_k, 0);
+    if (ce == cudaSuccess && readback)
+        ce = cudaMemcpyAsync(sl.h_res, sl.d_res, (size_t)sl.total * 5, cudaMemcpyDeviceToHost, s->down);
+    if (ce == cudaSuccess) ce = cudaEventRecord(sl.ev, s->down);
+    return ce == cudaSuccess ? MC_OK : mc_cuda_fail(ce, "server: results read-back");
 }
 
 void launcher_main(mc_server* s) {
@@ -341,8 +357,8 @@ void launcher_main(mc_server* s) {
         }
         Slot& sl = s->slots[si];
         int rc = run_batch(s, sl, reqs);
-        cudaError_t ce = cudaEventRecord(sl.ev, s->stream);
-        if (rc == MC_OK && ce != cudaSuccess) rc = MC_ERR_CUDA;
+        const int rc_fin = finish_batch(s, sl, rc == MC_OK && sl.step_launch);
+        if (rc == MC_OK) rc = rc_fin;
         for (Req* r : reqs)
             if (rc != MC_OK) r->status = rc;
         std::lock_guard<std::mutex> lk(s->mu);
@@ -511,11 +527,15 @@ extern "C" int mc_server_create(const mc_server_config* cfg, mc_server** out) {
     if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->admit_stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaMalloc(&s->flags, MC_FLAG_WORDS * sizeof(int32_t));
     if (ce == cudaSuccess) ce = cudaMemset(s->flags, 0, MC_FLAG_WORDS * sizeof(int32_t));
     for (int i = 0; i < s->nslots && ce == cudaSuccess; ++i) {
         Slot& sl = s->slots[i];
         ce = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&sl.ev_up, cudaEventDisableTiming);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&sl.ev_k, cudaEventDisableTiming);
         if (ce == cudaSuccess) ce = cudaMallocHost(&sl.h_act, (size_t)s->cap);
         if (ce == cudaSuccess) ce = cudaMalloc(&sl.d_act, (size_t)s->cap);
         if (ce == cudaSuccess) ce = cudaMallocHost(&sl.h_res, (size_t)s->cap * 5);
@@ -555,6 +575,8 @@ extern "C" int mc_server_destroy(mc_server* s) {
     for (int i = 0; i < s->nslots; ++i) {
         Slot& sl = s->slots[i];
         if (sl.ev) cudaEventDestroy(sl.ev);
+        if (sl.ev_up) cudaEventDestroy(sl.ev_up);
+        if (sl.ev_k) cudaEventDestroy(sl.ev_k);
         if (sl.h_act) cudaFreeHost(sl.h_act);
         if (sl.d_act) cudaFree(sl.d_act);
         if (sl.h_res) cudaFreeHost(sl.h_res);
@@ -562,6 +584,8 @@ extern "C" int mc_server_destroy(mc_server* s) {
     }
     if (s->flags) cudaFree(s->flags);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->up) cudaStreamDestroy(s->up);
+    if (s->down) cudaStreamDestroy(s->down);
     if (s->admit_stream) cudaStreamDestroy(s->admit_stream);
     delete s;
     return MC_OK;
