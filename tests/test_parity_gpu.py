@@ -22,12 +22,16 @@ PLAIN, FUSED = capi.FORM_PLAIN, capi.FORM_FUSED
 
 
 def run_vs_oracle(cuda, steps, seed, form, obs_dtype="uint8", B=64, world=16, res=(32, 32), stage=None,
-                  break_half=False, look_delta=0.1, episode_length=None, world_xyz=None, reset_every=None, **kw):
+                  break_half=False, look_delta=0.1, episode_length=None, world_xyz=None, reset_every=None,
+                  fused_cfg=None, debug=True, **kw):
     wx, wy, wz = world_xyz or (world, world, world)
     g = GpuEnv(cuda, B, world_x=wx, world_y=wy, world_z=wz, render_width=res[0], render_height=res[1],
-               obs_dtype=obs_dtype, numerics="ieee", look_delta=look_delta, episode_length=episode_length, **kw)
+               obs_dtype=obs_dtype, numerics="ieee", look_delta=look_delta, episode_length=episode_length,
+               debug=debug, **kw)
     if stage is not None:
         g.set_fused(stage)
+    if fused_cfg is not None:
+        g.set_fused(*fused_cfg)
     o = O.OracleEnv(batch_size=B, world_x=wx, world_y=wy, world_z=wz, render_width=res[0], render_height=res[1],
                     obs_dtype=obs_dtype, debug=True, episode_length=episode_length, **kw)
     g.reset()
@@ -98,6 +102,51 @@ def test_small_and_odd_sizes(cuda, form):
 @pytest.mark.parametrize("mode", ["uint8", "uint8_prebasis"])
 def test_noncubic_world_bit_exact(cuda, mode):
     run_vs_oracle(cuda, 25, 8, FUSED, obs_dtype=mode, B=17, world_xyz=(24, 16, 20), res=(16, 16))
+
+
+# Shapes for the march without debug outputs (kwargs of run_vs_oracle).
+EARLY_EXIT_CASES = {
+    "c1": dict(steps=30, seed=0, B=40),
+    "one_env_8cube_7x5": dict(steps=25, seed=6, B=1, world=8, res=(7, 5)),
+    "world5_f32": dict(steps=25, seed=7, B=3, world=5, res=(16, 16), obs_dtype="float32"),
+    "noncubic": dict(steps=25, seed=8, B=17, world_xyz=(24, 16, 20), res=(16, 16)),
+    "w32_64x64_break": dict(steps=12, seed=2, B=24, world=32, res=(64, 64), break_half=True),
+    "steps3_vd2.5": dict(steps=10, seed=9, B=9, max_steps=3, view_distance=2.5),
+    "steps20_vd6": dict(steps=15, seed=10, B=30, max_steps=20, view_distance=6.0),
+    "episodes_masked_reset": dict(steps=45, seed=4, B=50, episode_length=9, reset_every=13, break_half=True),
+    "wide_flat_32x8x32": dict(steps=20, seed=12, B=21, world_xyz=(32, 8, 32), res=(8, 8), ground_height=4,
+                              break_half=True),
+}
+
+
+@pytest.mark.parametrize("case", sorted(EARLY_EXIT_CASES))
+@pytest.mark.parametrize("mode", ["uint8", "uint8_minimal"])
+@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1)], ids=["per_warp", "team"])
+def test_early_exit_march_vs_oracle(cuda, case, mode, cfg):
+    """The fused kernels without debug outputs, where the march over a
+    staged world ends rays early (left the box, above the highest solid
+    layer, view distance tested at the hit) in PTX loops, against the CPU
+    oracle: bit-exact on every state field and observation byte."""
+    kw = dict(EARLY_EXIT_CASES[case])
+    kw.setdefault("obs_dtype", mode)
+    wx, wy, wz = kw.get("world_xyz") or (kw.get("world", 16),) * 3
+    if (wx * wy * wz) % 16:
+        cfg = (0,) + tuple(cfg[1:])  # a bulk copy needs whole 16-byte chunks: march the global world
+    elif cfg[4] == 1 and wx * wy * wz > 16384:
+        cfg = (1, 4, 1, 4, 1, 0)  # one 32 KB world per warp: 4 warps fit in a CTA's shared memory
+    run_vs_oracle(cuda, kw.pop("steps"), kw.pop("seed"), FUSED, fused_cfg=cfg, debug=False, **kw)
+
+
+@pytest.mark.parametrize("mode", ["uint8", "uint8_minimal"])
+@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1)], ids=["per_warp", "team"])
+def test_wide_flat_world_staged(cuda, mode, cfg):
+    """A 32x8x32 world (1 KB layers) with 8x8 images, staged: the march
+    loads one voxel past the box before its exit test, and the layouts keep
+    one world layer allocated in front of the first staged world and after
+    the last; here the tables and bands in front of the first world are
+    shorter than a layer, so both layouts add that room."""
+    run_vs_oracle(cuda, 20, 12, FUSED, obs_dtype=mode, B=21, world_xyz=(32, 8, 32), res=(8, 8), ground_height=4,
+                  break_half=True, fused_cfg=cfg)
 
 
 def test_limits_max_steps_and_view_distance(cuda):
