@@ -596,6 +596,19 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
     return b;
 }
 
+// Start values of march_packed_shared for an env whose eye is in voxel
+// (vx, vy, vz), one per sign combination k of the ray (bit 0: x >= 0, bit 1:
+// y >= 0, bit 2: z >= 0): {packed index and counts, x, y and z increments}.
+__device__ __forceinline__ int4 packed_start(int k, int vx, int vy, int vz, int wx, int wy, int wz, int ytop) {
+    const int sx = (k & 1) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 4) ? 1 : -1;
+    const int wxz = wx * wz, idx = vy * wxz + vx * wz + vz;
+    // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+    const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+              cz = (sz > 0) ? wz - 1 - vz : vz;
+    return make_int4((idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz),
+                     ((sx * wz) << 18) + (1 << 12), ((sy * wxz) << 18) + (1 << 6), (sz << 18) + 1);
+}
+
 // Counts of the split march: three 7-bit in-box step counts (z bits 0-6,
 // x 7-13, y 14-20) that count up from 63 - (steps left) and set bit 6 of
 // their field on leaving the box, and a 9-bit step count (bits 21-29) that
@@ -731,11 +744,14 @@ __device__ __forceinline__ float aabb_exit(float ix, float iy, float iz, float l
 // VDLIM = false leaves out the branch-free march for view-limited worlds
 // (those then take the reference-shaped loop), for callers whose register
 // budget is better spent elsewhere.
-template <bool FASTG, class V, bool VDLIM = true>
+// TAB: the caller passes `start`, the packed march's start values for the
+// eight sign combinations of the ray (packed_starts), whenever the packed
+// march applies to the env (nullptr otherwise).
+template <bool FASTG, class V, bool VDLIM = true, bool TAB = false>
 __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                          int wz, int max_steps, float vd, int gh, bool inside,
                                          bool skip_first = false, bool sky_exit = false, bool vd_safe = false,
-                                         int ytop = 1 << 20) {
+                                         int ytop = 1 << 20, const int4* start = nullptr) {
     float ray_x, ray_y, ray_z;
     ray_dir<true>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::sqrt(len2(ray_x, ray_y, ray_z));
@@ -796,7 +812,12 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                       cz = (sz > 0) ? wz - 1 - vz : vz;
             if (b < 0) {
                 const uint32_t base = (uint32_t)__cvta_generic_to_shared(vox.w);
-                if (vd_safe && max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
+                if (TAB && start) {
+                    // the env's start values for this ray's signs
+                    const int4 e = start[(ray_x >= 0.0f ? 1 : 0) | (ray_y >= 0.0f ? 2 : 0) | (ray_z >= 0.0f ? 4 : 0)];
+                    b = march_packed_shared(base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz);
+                } else if (vd_safe && max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 &&
+                           wx * wy * wz < 8192) {
                     // index and in-box counts in one register (march_packed_shared)
                     const int packed = (idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz);
                     b = march_packed_shared(base, packed, (dix << 18) + (1 << 12), (diy << 18) + (1 << 6),
@@ -1424,12 +1445,12 @@ __host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int 
     L.tile_h = 32 / tile_w;
     L.stage_bytes = mc_align16(W * L.tile_h * 3 * (obs_f32 ? 4 : 1));
     L.world_bytes = stage ? mc_align16(wxyz) : 0;
-    L.warp_bytes = 16 + L.stage_bytes + L.world_bytes;  // 16: mbarrier
+    L.warp_bytes = 16 + 128 + L.stage_bytes + L.world_bytes;  // 16: mbarrier, 128: packed_start table
     L.head_bytes = mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
     // the march reads up to wx*wz bytes on either side of a staged world:
     // keep that much allocated before the first world and after the last
     L.pad_bytes = stage ? mc_align16(wxz) : 0;
-    const int before = L.head_bytes + 16 + L.stage_bytes;
+    const int before = L.head_bytes + 16 + 128 + L.stage_bytes;
     if (before < L.pad_bytes) L.head_bytes += mc_align16(L.pad_bytes - before);
     return L;
 }
@@ -1648,8 +1669,9 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
     }
     uint8_t* wbase = smem + L.head_bytes + warp * L.warp_bytes;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(wbase);
-    uint8_t* stage = wbase + 16;
-    int8_t* sworld = reinterpret_cast<int8_t*>(wbase + 16 + L.stage_bytes);
+    int4* sstart = reinterpret_cast<int4*>(wbase + 16);
+    uint8_t* stage = wbase + 16 + 128;
+    int8_t* sworld = reinterpret_cast<int8_t*>(wbase + 16 + 128 + L.stage_bytes);
     uint32_t mbar_a = smem_u32(mbar);
     if (STAGE && lane == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
@@ -1825,6 +1847,15 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
         const bool sky_exit = (FAM == MC_FAM_SHADED) ? (inside && p.vd > 0.0f && !p.dbg_pixel)
                                                      : (eye_inb && !p.dbg_pixel);
         const bool vd_safe = sky_exit && box_within_view(c, p.wx, p.wy, p.wz, p.vd);
+        // where every ray takes the packed march, its start values per sign
+        // combination, built once for the env
+        const int4* start = nullptr;
+        if (STAGE && FAM == MC_FAM_SHADED && vd_safe && p.max_steps > p.wx + p.wy + p.wz && p.wx <= 31 &&
+            p.wy <= 31 && p.wz <= 31 && wxyz < 8192) {
+            if (lane < 8) sstart[lane] = packed_start(lane, d0.vx, d0.vy, d0.vz, p.wx, p.wy, p.wz, ytop);
+            __syncwarp();
+            start = sstart;
+        }
         const int TW = L.tile_w, TH = L.tile_h;
         const int lx = lane % TW, ly = lane / TW;
         const int bpp = 3 * (F32 ? 4 : 1);  // bytes per pixel
@@ -1839,7 +1870,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         // the one-warp-per-env kernel keeps its 64-register budget: the
                         // branch-free march only where the whole box is within view
-                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxShared, false>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe, ytop);
+                        if (STAGE) h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxShared, false, true>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe, ytop, start);
                         else h = shade_ray<FAM == MC_FAM_SHADED_FAST, VoxGlobal, false>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh, inside, skip_first, sky_exit, vd_safe);
                     } else if (FAM == MC_FAM_FP16) {
                         if (STAGE) h = fp16_ray(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
