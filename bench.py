@@ -307,6 +307,25 @@ def run_mine(args):
     e2e_value = B * K * world / t_e2e
     _ = float(h_rew.sum())
 
+    # the reference's published headline configuration is this shape with
+    # float32 observations (49.6 M env-steps/s on an RTX 3090): the same
+    # trajectory window with float32 observations, for comparison
+    f32 = None
+    if args.workload == "peak" and not args.shape and saved is None:
+        env32 = MineEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                        device=str(dev), max_steps=W["max_steps"], obs_dtype="float32", numerics="ref_fast",
+                        form="fused", look_delta=W["look_delta"])
+        env32.reset()
+        if Wm:
+            env32.rollout(acts_w)
+        env32.prepare_rollout(acts_t)
+        t32 = timed(lambda: env32.rollout(acts_t))
+        env32.check_error()
+        f32 = {"obs_dtype": "float32", "value": B * K * world / t32, "unit": "env-steps/s",
+               "ms_per_step": t32 / K * 1e3, "published_rtx3090": 49.6e6,
+               "note": "the reference's published number is float32 obs on an RTX 3090 (README.md:11,50)"}
+        del env32
+
     peak, peak_kind = load_peaks()
     achieved = bytes_per_env_step * B / (t_fused / K) / 1e9
     line = {
@@ -342,6 +361,8 @@ def run_mine(args):
         "gpu_launches": K,
         "clocks": clk.summary(),
     }
+    if f32 is not None:
+        line["float32_obs"] = f32
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B=min(2048, B // 2) if B > 1 else 1, W=W)
     if rank == 0:
