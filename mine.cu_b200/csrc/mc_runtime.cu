@@ -144,7 +144,11 @@ __global__ void k_regen(int8_t* vox, const int8_t* tmpl, int B, int wxyz, int32_
     __shared__ int go;
     if (threadIdx.x == 0) go = conditional ? (*(volatile int32_t*)&flags[MC_FLAG_ANY_DONE] != 0) : 1;
     __syncthreads();
-    if (go) {
+    // The flag was set before this launch and only its last CTA clears it,
+    // after every CTA has read it: all CTAs read the same value, so when it
+    // is clear none of them has anything to write, count or clear.
+    if (!go) return;
+    {
         if ((wxyz & 15) == 0) {
             const int n16 = wxyz >> 4;
             const uint4* t4 = reinterpret_cast<const uint4*>(tmpl);
