@@ -1055,10 +1055,13 @@ __device__ __forceinline__ uint32_t to_u8(float x) {
 // caller needs only the colour of sky pixels) the march stops when the ray
 // leaves the box, where the reference keeps stepping out-of-box voxels until
 // max_steps: a ray that left never re-enters, so both end as sky.
-template <bool TRIG, class V>
+// TAB: `start` holds the packed march's start values per ray sign
+// combination (packed_start) whenever every ray of the env takes the packed
+// march, else nullptr.
+template <bool TRIG, class V, bool TAB = false>
 __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, float v, const V& vox, int wx, int wy,
                                         int wz, int max_steps, bool skip_first = false, bool sky_exit = false,
-                                        int ytop = 1 << 20) {
+                                        int ytop = 1 << 20, const int4* start = nullptr) {
     float ray_x, ray_y, ray_z;
     ray_dir<TRIG>(c, u, v, ray_x, ray_y, ray_z);
     float ray_len = N::rsqrt(len2(ray_x, ray_y, ray_z));
@@ -1092,8 +1095,13 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
             // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
             const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
                       cz = (sz > 0) ? wz - 1 - vz : vz;
-            b = march_staged(staged_base(vox), idx, cx, cy, cz, dix, diy, diz, wx, wy, wz, max_steps, tmx, tmy, tmz,
-                             tdx, tdy, tdz);
+            if (TAB && start) {
+                const int4 e = start[(ray_x >= 0.0f ? 1 : 0) | (ray_y >= 0.0f ? 2 : 0) | (ray_z >= 0.0f ? 4 : 0)];
+                b = march_packed_shared(staged_base(vox), e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz);
+            } else {
+                b = march_staged(staged_base(vox), idx, cx, cy, cz, dix, diy, diz, wx, wy, wz, max_steps, tmx, tmy,
+                                 tmz, tdx, tdy, tdz);
+            }
             if (b >= 0) {
                 const bool bx = tmx < tmy && tmx < tmz;
                 face = bx ? 0 : ((tmy < tmz) ? 1 : 2);
@@ -1850,8 +1858,9 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
         // where every ray takes the packed march, its start values per sign
         // combination, built once for the env
         const int4* start = nullptr;
-        if (STAGE && FAM == MC_FAM_SHADED && vd_safe && p.max_steps > p.wx + p.wy + p.wz && p.wx <= 31 &&
-            p.wy <= 31 && p.wz <= 31 && wxyz < 8192) {
+        const bool flat_fam = FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS;
+        if (STAGE && (FAM == MC_FAM_SHADED ? vd_safe : (flat_fam && sky_exit)) &&
+            p.max_steps > p.wx + p.wy + p.wz && p.wx <= 31 && p.wy <= 31 && p.wz <= 31 && wxyz < 8192) {
             if (lane < 8) sstart[lane] = packed_start(lane, d0.vx, d0.vy, d0.vz, p.wx, p.wy, p.wz, ytop);
             __syncwarp();
             start = sstart;
@@ -1877,7 +1886,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                         else h = fp16_ray(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps);
                     } else {
                         constexpr bool TRIG = (FAM != MC_FAM_PREBASIS);
-                        if (STAGE) h = flat_ray<TRIG>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit, ytop);
+                        if (STAGE) h = flat_ray<TRIG, VoxShared, true>(c, d0, u, v, VoxShared{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit, ytop, start);
                         else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
                     }
                     const int so = ly * W + px;  // pixel within the staged band
