@@ -171,6 +171,19 @@ int mc_env_render(mc_env* env, void* stream);
  * shards of a batch split over several GPUs, with *flag the all-reduced
  * any-done byte. */
 int mc_env_regenerate_if(mc_env* env, const uint8_t* flag, void* stream);
+/* Which worlds a step's dones (and reset(mask)) regenerate.  MC_REGEN_ALL,
+ * the default: every world when any env is done or reset, the reference's
+ * rule (minecu/__init__.py:290-300, 356-358, 439-441).  MC_REGEN_PER_ENV
+ * (opt-in): only the worlds of the envs done or reset; the other envs keep
+ * their worlds.  The reference has this only as unused masked kernels
+ * (src/kernels.cu:1988-2069), which also leave out the house; here a
+ * regenerated world is the start world, house included.  Setting the mode
+ * drops the env's cached rollout graphs. */
+#define MC_REGEN_ALL 0
+#define MC_REGEN_PER_ENV 1
+int mc_env_set_regen_mode(mc_env* env, int32_t mode);
+/* The mode, or a negative status. */
+int mc_env_get_regen_mode(const mc_env* env);
 /* K fused steps of discrete actions actions[K,B] captured once in a CUDA
  * graph and replayed; rewards_out / dones_out ([K,B], optional) receive each
  * step's rewards and dones.  The graph is cached per (actions, outputs, K). */

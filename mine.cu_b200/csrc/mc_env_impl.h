@@ -46,6 +46,7 @@ struct mc_env {
     cudaStream_t cap_stream;
     std::vector<RolloutGraph> graphs;
     HostIO* hio;
+    int regen_mode;  // MC_REGEN_ALL (the reference's rule) or MC_REGEN_PER_ENV
 };
 
 // Record a formatted message for mc_last_error() and return `code`.

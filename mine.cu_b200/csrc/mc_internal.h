@@ -46,6 +46,7 @@ struct mc_kp {
     int family;   // MC_FAM_*
     int obs_f32;  // float32 obs (else uint8)
     float look_delta;  // discrete-action look step (radians)
+    int regen_per_env; // MC_REGEN_PER_ENV: a done (or reset) env regenerates only its own world
     // state (device, borrowed from the caller)
     int8_t* voxels;
     float* positions;

@@ -257,8 +257,34 @@ int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s) 
     return (int)cudaGetLastError();
 }
 
+// Per-env regeneration (MC_REGEN_PER_ENV): the world of every env whose
+// do_reset is set this step is copied from the template, the others are left
+// alone; the all-world rule's flag is cleared unused.  The rule of the
+// reference's unused masked kernels (src/kernels.cu:1988-2069), except that
+// the template also holds the house, as every world does at the start.
+__global__ void k_regen_masked(int8_t* vox, const int8_t* tmpl, const uint8_t* do_reset, int B, int wxyz,
+                               int32_t* flags) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) flags[MC_FLAG_ANY_DONE] = 0;
+    for (long long b = blockIdx.x; b < B; b += gridDim.x) {
+        if (!do_reset[b]) continue;  // the same value for every thread of the CTA
+        if ((wxyz & 15) == 0) {
+            uint4* d4 = reinterpret_cast<uint4*>(vox + b * (long long)wxyz);
+            const uint4* t4 = reinterpret_cast<const uint4*>(tmpl);
+            for (int k = threadIdx.x; k < (wxyz >> 4); k += blockDim.x) d4[k] = __ldg(t4 + k);
+        } else {
+            int8_t* d = vox + b * (long long)wxyz;
+            for (int k = threadIdx.x; k < wxyz; k += blockDim.x) d[k] = tmpl[k];
+        }
+    }
+}
+
 int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s) {
     int wxyz = p->wx * p->wy * p->wz;
+    if (conditional && p->regen_per_env) {
+        const int grid = p->B < 1184 ? (p->B > 0 ? p->B : 1) : 1184;
+        k_regen_masked<<<grid, 256, 0, s>>>(p->voxels, p->world_template, p->do_reset, p->B, wxyz, p->flags);
+        return (int)cudaGetLastError();
+    }
     int grid = p->B < 1184 ? (p->B > 0 ? p->B : 1) : 1184;  // 148 SMs x 8
     k_regen<<<grid, 256, 0, s>>>(p->voxels, p->world_template, p->B, wxyz, p->flags, conditional);
     return (int)cudaGetLastError();
@@ -657,6 +683,7 @@ extern "C" int mc_env_set_state(mc_env* e, const mc_env_state* s) {
     fill_kp(&e->kp, &e->cfg, s);
     e->kp.flags = flags;
     e->kp.world_template = tmpl;
+    e->kp.regen_per_env = e->regen_mode == MC_REGEN_PER_ENV;
     e->kp.sched_dynamic = 1;
     drop_graphs(e);
     return MC_OK;
@@ -846,6 +873,20 @@ extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* h
 extern "C" int mc_env_host_join(mc_env* e, void* stream) {
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     return hostio_join(e->hio, (cudaStream_t)stream);
+}
+
+extern "C" int mc_env_set_regen_mode(mc_env* e, int32_t mode) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    if (mode != MC_REGEN_ALL && mode != MC_REGEN_PER_ENV) return fail(MC_ERR_INVALID, "unknown regen mode %d", mode);
+    e->regen_mode = mode;
+    e->kp.regen_per_env = mode == MC_REGEN_PER_ENV;
+    drop_graphs(e);  // captured steps hold the old rule
+    return MC_OK;
+}
+
+extern "C" int mc_env_get_regen_mode(const mc_env* e) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    return e->regen_mode;
 }
 
 extern "C" int mc_env_regenerate_if(mc_env* e, const uint8_t* flag, void* stream) {

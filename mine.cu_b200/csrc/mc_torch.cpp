@@ -497,6 +497,8 @@ void env_host_join(std::shared_ptr<Env> e) { ck(mc_env_host_join(e->h, cur_strea
 
 void env_render(std::shared_ptr<Env> e) { ck(mc_env_render(e->h, cur_stream()), "render"); }
 
+void env_set_regen_mode(std::shared_ptr<Env> e, int mode) { ck(mc_env_set_regen_mode(e->h, mode), "set_regen_mode"); }
+
 void env_regenerate_if(std::shared_ptr<Env> e, torch::Tensor flag) {
     TORCH_CHECK(flag.is_cuda() && flag.numel() >= 1 && flag.element_size() == 1,
                 "flag must be a one-byte CUDA tensor (uint8 or bool)");
@@ -723,6 +725,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("env_step_host", &env_step_host);
     m.def("env_host_join", &env_host_join);
     m.def("env_render", &env_render);
+    m.def("env_set_regen_mode", &env_set_regen_mode);
     m.def("env_regenerate_if", &env_regenerate_if);
     m.def("env_rollout", &env_rollout, py::arg("env"), py::arg("actions"), py::arg("rewards_out") = py::none(),
           py::arg("dones_out") = py::none());

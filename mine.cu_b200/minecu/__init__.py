@@ -48,7 +48,7 @@ except (ImportError, OSError) as exc:  # fail loudly: there is no fallback
 from minecu.config import EnvConfig, TrainConfig, DEFAULT_ENV, FAST_ENV, QUALITY_ENV  # noqa: E402
 
 __version__ = "0.2.0"
-__all__ = ["MineEnv", "BlockType", "EnvConfig", "TrainConfig", "OBS_MODES", "NUMERICS", "lib_path"]
+__all__ = ["MineEnv", "BlockType", "EnvConfig", "TrainConfig", "OBS_MODES", "NUMERICS", "REGEN_MODES", "lib_path"]
 
 # obs_dtype -> C-ABI MC_OBS_* (include/minecu_b200.h); the reference accepts
 # the first seven (minecu/__init__.py:167-169), uint8_fast exposes its
@@ -63,6 +63,9 @@ OBS_MODES = {
     "uint8_smem": 6,
     "uint8_fast": 7,
 }
+
+# which worlds dones and masked resets regenerate (C-ABI MC_REGEN_*)
+REGEN_MODES = {"all": 0, "per_env": 1}
 NUMERICS = {"ref_fast": 0, "ieee": 1}
 FORMS = {"plain": 0, "fused": 1}
 
@@ -165,6 +168,7 @@ class MineEnv:
         form: str = "fused",
         look_delta: float = 0.1,
         debug: bool = False,
+        regen: str = "all",
     ):
         assert "cuda" in str(device), "MineEnv requires CUDA device"
         if obs_dtype not in OBS_MODES:
@@ -173,6 +177,8 @@ class MineEnv:
             raise ValueError(f"numerics must be one of {sorted(NUMERICS)}")
         if form not in FORMS:
             raise ValueError(f"form must be one of {sorted(FORMS)}")
+        if regen not in REGEN_MODES:
+            raise ValueError(f"regen must be one of {sorted(REGEN_MODES)}")
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -215,6 +221,8 @@ class MineEnv:
         with torch.cuda.device(self.device):
             self._env = _C.env_create(self._config_dict(), self._state_dict_ptrs())
             self._generate_world()
+        self.regen = "all"
+        self.set_regen(regen)
 
     # ------------------------------------------------------------------
     def _config_dict(self) -> dict:
@@ -352,6 +360,16 @@ class MineEnv:
         with torch.cuda.device(self.device):
             _C.env_render(self._env)
         return self.obs_buffer
+
+    def set_regen(self, mode: str) -> None:
+        """Which worlds a step's dones (and reset(mask)) regenerate: "all"
+        (the reference's rule: every world when any env is done or reset) or
+        "per_env" (opt-in: only the worlds of the envs done or reset, each
+        back to the start world)."""
+        if mode not in REGEN_MODES:
+            raise ValueError(f"regen must be one of {sorted(REGEN_MODES)}")
+        _C.env_set_regen_mode(self._env, REGEN_MODES[mode])
+        self.regen = mode
 
     def regenerate_if(self, flag: torch.Tensor) -> None:
         """Regenerate every world when the one-byte device tensor `flag` is

@@ -111,6 +111,8 @@ _PROTOS = {
     "mc_env_step_host": (I, [P, P, P, P, ctypes.c_int, P]),
     "mc_env_host_join": (I, [P, P]),
     "mc_env_render": (I, [P, P]),
+    "mc_env_set_regen_mode": (I, [P, ctypes.c_int32]),
+    "mc_env_get_regen_mode": (I, [P]),
     "mc_env_regenerate_if": (I, [P, P, P]),
     "mc_env_rollout": (I, [P, P, I, P, P, P]),
     "mc_env_rollout_prepare": (I, [P, P, I, P, P]),

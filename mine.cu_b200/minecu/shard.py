@@ -63,7 +63,8 @@ class ShardedEnv:
             raise ValueError(f"rank {self.rank} holds envs [{self.start}, {self.start + self.count}); "
                              f"its env has batch_size {n}")
         self.global_batch = global_batch
-        self.sync_regen = sync_regen and self.world > 1
+        # per-env regeneration couples no envs: nothing to all-reduce
+        self.sync_regen = sync_regen and self.world > 1 and getattr(env, "regen", "all") == "all"
         self.flag_device = flag_device if flag_device is not None else getattr(env, "device", torch.device("cpu"))
         self._flag = torch.zeros(1, dtype=torch.uint8, device=self.flag_device)
 

@@ -129,6 +129,19 @@ static void regen_all(const orc_cfg* c, orc_state* s) {
     orc_place_house(s->voxels, c->B, c->wx, c->wy, c->wz, c->house_x, c->house_z, c->ground_height);
 }
 
+/* The per-env rule (regen_per_env): the same three generators on the world
+ * of each env whose do_reset is set, the others untouched. */
+static void regen_flagged(const orc_cfg* c, orc_state* s) {
+    const long long wxyz = (long long)c->wx * c->wy * c->wz;
+    for (long long i = 0; i < c->B; ++i) {
+        if (!s->do_reset[i]) continue;
+        int8_t* w = s->voxels + i * wxyz;
+        orc_generate_world(w, 1, c->wx, c->wy, c->wz, c->ground_height);
+        orc_place_tree(w, 1, c->wx, c->wy, c->wz, c->tree_x, c->tree_z, c->ground_height);
+        orc_place_house(w, 1, c->wx, c->wy, c->wz, c->house_x, c->house_z, c->ground_height);
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Render                                                              */
 /* ------------------------------------------------------------------ */
@@ -584,7 +597,8 @@ int orc_env_step(const orc_cfg* c, orc_state* s, const int8_t* buttons, const fl
     }
     int n_done = 0;
     for (i = 0; i < c->B; ++i) n_done += s->do_reset[i];
-    if (any_done) regen_all(c, s);
+    if (c->regen_per_env) regen_flagged(c, s);
+    else if (any_done) regen_all(c, s);
     return n_done;
 }
 
@@ -612,7 +626,8 @@ void orc_env_reset(const orc_cfg* c, orc_state* s, const uint8_t* mask, int thre
             s->step_count[i] = 0;
         }
     }
-    if (mask == NULL || any) regen_all(c, s);
+    if (c->regen_per_env) regen_flagged(c, s);
+    else if (mask == NULL || any) regen_all(c, s);
     orc_env_render(c, s, threads);
 }
 

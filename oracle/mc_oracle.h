@@ -45,6 +45,8 @@ typedef struct orc_cfg {
     int has_limit, episode_length;
     int render;                 /* ORC_RENDER_* used by step() */
     int obs_f32;                /* 1: float32 obs, 0: uint8 obs */
+    int regen_per_env;          /* 1: a done or reset env regenerates only its own world (the
+                                   build's opt-in MC_REGEN_PER_ENV); 0: every world, the reference's rule */
 } orc_cfg;
 
 typedef struct orc_state {

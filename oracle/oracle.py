@@ -48,7 +48,7 @@ class OrcCfg(ctypes.Structure):
         ("tree_x", ctypes.c_int), ("tree_z", ctypes.c_int),
         ("house_x", ctypes.c_int), ("house_z", ctypes.c_int),
         ("episode_rule", ctypes.c_int), ("has_limit", ctypes.c_int), ("episode_length", ctypes.c_int),
-        ("render", ctypes.c_int), ("obs_f32", ctypes.c_int),
+        ("render", ctypes.c_int), ("obs_f32", ctypes.c_int), ("regen_per_env", ctypes.c_int),
     ]
 
 
@@ -108,7 +108,7 @@ class OracleEnv:
                  render_width=64, render_height=64, max_steps=64, view_distance=32.0,
                  fov_degrees=70.0, dt=0.05, gravity=-20.0, walk_speed=4.0, sprint_mult=1.5,
                  jump_vel=8.0, ground_height=8, target_block=3, reward_value=1.0,
-                 episode_length=None, seed=42, obs_dtype="float32", debug=False, threads=0):
+                 episode_length=None, seed=42, obs_dtype="float32", debug=False, threads=0, regen="all"):
         self.B = batch_size
         self.wx = world_x if world_x is not None else world_size
         self.wy = world_y if world_y is not None else world_size
@@ -134,6 +134,7 @@ class OracleEnv:
         else:
             c.has_limit, c.episode_length = (0, 0) if episode_length is None else (1, episode_length)
         c.render, c.obs_f32 = fam, int(f32)
+        c.regen_per_env = 1 if regen == "per_env" else 0
         self.cfg = c
         B = self.B
         self.voxels = np.zeros((B, self.wy, self.wx, self.wz), np.int8)

@@ -63,6 +63,10 @@ class GpuEnv:
         except Exception:
             pass
 
+    def set_regen(self, per_env: bool):
+        capi.check(capi.lib().mc_env_set_regen_mode(self.h, 1 if per_env else 0), "set_regen_mode")
+        assert capi.lib().mc_env_get_regen_mode(self.h) == (1 if per_env else 0)
+
     def set_fused(self, stage, warps_per_cta=8, ctas_per_sm=4, tile_w=8, team_warps=1, coop=0):
         f = capi.FusedConfig(stage, warps_per_cta, ctas_per_sm, tile_w, team_warps, coop)
         capi.check(capi.lib().mc_env_set_fused_config(self.h, ctypes.byref(f)), "set_fused_config")

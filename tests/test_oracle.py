@@ -169,3 +169,30 @@ def test_discrete_adapter_table():
     assert list(look[7]) == [0.25, 0] and list(look[8]) == [-0.25, 0]
     assert list(look[9]) == [0, 0.25] and list(look[10]) == [0, -0.25]
     assert btn[11].sum() == 0 and (look[11] == 0).all()
+
+
+def test_per_env_regen_rule_on_masked_reset():
+    """The oracle's per-env rule (the build's opt-in MC_REGEN_PER_ENV): a
+    masked reset returns only the masked envs' worlds to the start world;
+    the other worlds keep the blocks broken in them.  Under the reference's
+    rule every world returns to the start world."""
+    import numpy as np
+    from mc_harness import actions_for
+    for regen in ("per_env", "all"):
+        e = O.OracleEnv(batch_size=6, world_size=16, render_width=8, render_height=8, obs_dtype="uint8",
+                        regen=regen)
+        e.reset()
+        start = e.voxels[0].copy()
+        for s in range(8):
+            _, btn, look = actions_for(6, s, 3, break_half=True)
+            e.step(btn, look)
+        before = e.voxels.copy()
+        changed = [i for i in range(6) if not np.array_equal(before[i], start)]
+        mask = np.array([1, 0, 1, 0, 0, 0], np.uint8)
+        assert any(not mask[i] for i in changed), "an unmasked env should have broken a block"
+        e.reset(mask)
+        for i in range(6):
+            if regen == "all" or mask[i]:
+                assert np.array_equal(e.voxels[i], start), (regen, i)
+            else:
+                assert np.array_equal(e.voxels[i], before[i]), (regen, i)

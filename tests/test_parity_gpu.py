@@ -23,7 +23,7 @@ PLAIN, FUSED = capi.FORM_PLAIN, capi.FORM_FUSED
 
 def run_vs_oracle(cuda, steps, seed, form, obs_dtype="uint8", B=64, world=16, res=(32, 32), stage=None,
                   break_half=False, look_delta=0.1, episode_length=None, world_xyz=None, reset_every=None,
-                  fused_cfg=None, debug=True, **kw):
+                  fused_cfg=None, debug=True, regen="all", **kw):
     wx, wy, wz = world_xyz or (world, world, world)
     g = GpuEnv(cuda, B, world_x=wx, world_y=wy, world_z=wz, render_width=res[0], render_height=res[1],
                obs_dtype=obs_dtype, numerics="ieee", look_delta=look_delta, episode_length=episode_length,
@@ -32,8 +32,10 @@ def run_vs_oracle(cuda, steps, seed, form, obs_dtype="uint8", B=64, world=16, re
         g.set_fused(stage)
     if fused_cfg is not None:
         g.set_fused(*fused_cfg)
+    if regen != "all":
+        g.set_regen(True)
     o = O.OracleEnv(batch_size=B, world_x=wx, world_y=wy, world_z=wz, render_width=res[0], render_height=res[1],
-                    obs_dtype=obs_dtype, debug=True, episode_length=episode_length, **kw)
+                    obs_dtype=obs_dtype, debug=True, episode_length=episode_length, regen=regen, **kw)
     g.reset()
     o.reset()
     d = diff_report(g.state(), oracle_state(o), ["voxels", "positions", "obs", "cameras", "do_reset", "step_count"])
@@ -135,6 +137,23 @@ def test_early_exit_march_vs_oracle(cuda, case, mode, cfg):
     elif cfg[4] == 1 and wx * wy * wz > 16384:
         cfg = (1, 4, 1, 4, 1, 0)  # one 32 KB world per warp: 4 warps fit in a CTA's shared memory
     run_vs_oracle(cuda, kw.pop("steps"), kw.pop("seed"), FUSED, fused_cfg=cfg, debug=False, **kw)
+
+
+@pytest.mark.parametrize("form", [PLAIN, FUSED])
+@pytest.mark.parametrize("debug", [True, False])
+def test_per_env_regen_vs_oracle(cuda, form, debug):
+    """Opt-in per-env regeneration (MC_REGEN_PER_ENV): with short episodes,
+    masked resets and half the actions breaking blocks, only the worlds of
+    the envs done or reset return to the start world; every other world
+    keeps its broken blocks.  Bit-exact against the oracle's per-env rule."""
+    run_vs_oracle(cuda, 45, 14, form, B=50, episode_length=9, reset_every=13, break_half=True, regen="per_env",
+                  debug=debug)
+
+
+@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1)], ids=["per_warp", "team"])
+def test_per_env_regen_fused_configs(cuda, cfg):
+    run_vs_oracle(cuda, 30, 15, FUSED, B=33, episode_length=7, break_half=True, regen="per_env", debug=False,
+                  fused_cfg=cfg)
 
 
 @pytest.mark.parametrize("mode", ["uint8", "uint8_minimal"])
