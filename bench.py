@@ -307,6 +307,26 @@ def run_mine(args):
     e2e_value = B * K * world / t_e2e
     _ = float(h_rew.sum())
 
+    # the policy input a trainer takes (float32 NCHW obs / 255): one pass over
+    # the step's uint8 observation, timed on its own
+    policy = None
+    if W["obs_dtype"] != "float32":
+        pol_out = torch.empty((B, 3, W["res"], W["res"]), dtype=torch.float32, device=dev)
+        env.policy_obs(out=pol_out)
+        torch.cuda.synchronize()
+        n_pol = 20
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        for _ in range(n_pol):
+            env.policy_obs(out=pol_out)
+        e_b.record(stream)
+        torch.cuda.synchronize()
+        ms_pol = e_a.elapsed_time(e_b) / n_pol
+        pol_bytes = B * W["res"] ** 2 * 3 * 5  # uint8 read + float32 written
+        policy = {"ms": ms_pol, "GB_per_s": pol_bytes / (ms_pol * 1e-3) / 1e9, "layout": "NCHW float32 obs/255",
+                  "path": "MineEnv.policy_obs (mc_obs_to_policy)"}
+        del pol_out
+
     # the reference's published headline configuration is this shape with
     # float32 observations (49.6 M env-steps/s on an RTX 3090): the same
     # trajectory window with float32 observations, for comparison
@@ -363,6 +383,8 @@ def run_mine(args):
     }
     if f32 is not None:
         line["float32_obs"] = f32
+    if policy is not None:
+        line["policy_obs"] = policy
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B=min(2048, B // 2) if B > 1 else 1, W=W)
     if rank == 0:

@@ -411,6 +411,17 @@ int mc_philox_actions(uint8_t* actions, int32_t B, int32_t K, int32_t env_offset
 int mc_discrete_to_buttons(const uint8_t* actions, int32_t B, float look_delta, int8_t* buttons, float* look,
                            void* stream);
 
+/* ---- policy input: a uint8 observation as float32 in [0, 1] -----------
+ * The conversion a policy applies to the reference's observations before
+ * its first layer (examples/train_wood.py:51-56 permutes NHWC to NCHW), done
+ * in one pass: out = obs / 255 (IEEE division, correctly rounded) for every
+ * channel value of the uint8 [B,H,W,3] observation, written as float32
+ * [B,3,H,W] (MC_POLICY_NCHW) or [B,H,W,3] (MC_POLICY_NHWC).  No counterpart
+ * in the reference, whose observations are float32 by default. */
+#define MC_POLICY_NCHW 0
+#define MC_POLICY_NHWC 1
+int mc_obs_to_policy(const uint8_t* obs, float* out, int64_t B, int32_t H, int32_t W, int32_t layout, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1575,6 +1575,85 @@ extern "C" int mc_raycast_break(int8_t* vox, const float* pos, const float* yaw,
     return backend_rc(be->interact(&k, 1, (cudaStream_t)stream), "raycast_break");
 }
 
+namespace {
+// obs / 255 for every channel value; a thread converts 4 pixels at a time
+// when every env's pixel count is a multiple of 4 (then 12 bytes of input are
+// 4-byte aligned and each output plane segment is a float4), else 1 pixel.
+template <bool NCHW, int PX>
+__global__ void k_obs_to_policy(const uint8_t* __restrict__ obs, float* __restrict__ out, long long B, int HW) {
+    const long long groups = B * (HW / PX);
+    for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < groups;
+         gi += (long long)gridDim.x * blockDim.x) {
+        const long long b = gi / (HW / PX);
+        const int p0 = (int)(gi - b * (HW / PX)) * PX;
+        const long long pix = b * HW + p0;
+        float v[3 * PX];
+        if (PX == 4) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(obs + pix * 3);
+            const uint32_t w0 = src[0], w1 = src[1], w2 = src[2];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[k] = __fdiv_rn((float)((w0 >> (8 * k)) & 0xff), 255.0f);
+                v[4 + k] = __fdiv_rn((float)((w1 >> (8 * k)) & 0xff), 255.0f);
+                v[8 + k] = __fdiv_rn((float)((w2 >> (8 * k)) & 0xff), 255.0f);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3 * PX; ++k) v[k] = __fdiv_rn((float)obs[pix * 3 + k], 255.0f);
+        }
+        if (NCHW) {
+            // v holds PX pixels' RGB interleaved: channel c of pixel k is v[3k + c]
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float* plane = out + (b * 3 + c) * (long long)HW + p0;
+                if (PX == 4)
+                    *reinterpret_cast<float4*>(plane) = make_float4(v[c], v[3 + c], v[6 + c], v[9 + c]);
+                else
+                    plane[0] = v[c];
+            }
+        } else {
+            float* dst = out + pix * 3;
+            if (PX == 4) {
+                float4* d4 = reinterpret_cast<float4*>(dst);
+                d4[0] = make_float4(v[0], v[1], v[2], v[3]);
+                d4[1] = make_float4(v[4], v[5], v[6], v[7]);
+                d4[2] = make_float4(v[8], v[9], v[10], v[11]);
+            } else {
+                dst[0] = v[0];
+                dst[1] = v[1];
+                dst[2] = v[2];
+            }
+        }
+    }
+}
+}  // namespace
+
+extern "C" int mc_obs_to_policy(const uint8_t* obs, float* out, int64_t B, int32_t H, int32_t W, int32_t layout,
+                                void* stream) {
+    if (B < 0 || H < 0 || W < 0) return fail(MC_ERR_INVALID, "bad sizes");
+    if (layout != MC_POLICY_NCHW && layout != MC_POLICY_NHWC) return fail(MC_ERR_INVALID, "unknown layout %d", layout);
+    const long long HW = (long long)H * W;
+    if (B == 0 || HW == 0) return MC_OK;
+    if (HW > (1LL << 30)) return fail(MC_ERR_INVALID, "image too large");
+    if (!obs || !out) return fail(MC_ERR_INVALID, "NULL buffer");
+    const bool vec = (HW % 4) == 0 && (((uintptr_t)obs) & 3) == 0 && (((uintptr_t)out) & 15) == 0;
+    const long long groups = B * (vec ? HW / 4 : HW);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)std::min<long long>((groups + 255) / 256, (long long)sms * 16);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (layout == MC_POLICY_NCHW) {
+        if (vec) k_obs_to_policy<true, 4><<<grid, 256, 0, s>>>(obs, out, B, (int)HW);
+        else k_obs_to_policy<true, 1><<<grid, 256, 0, s>>>(obs, out, B, (int)HW);
+    } else {
+        if (vec) k_obs_to_policy<false, 4><<<grid, 256, 0, s>>>(obs, out, B, (int)HW);
+        else k_obs_to_policy<false, 1><<<grid, 256, 0, s>>>(obs, out, B, (int)HW);
+    }
+    MC_CK(cudaGetLastError());
+    return MC_OK;
+}
+
 extern "C" int mc_philox_actions(uint8_t* actions, int32_t B, int32_t K, int32_t env_offset, int32_t step0,
                                  uint64_t seed, int32_t break_half, void* stream) {
     if (B < 0 || K < 0) return fail(MC_ERR_INVALID, "bad sizes");

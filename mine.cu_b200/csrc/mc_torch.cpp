@@ -495,6 +495,17 @@ void env_step_host(std::shared_ptr<Env> e, torch::Tensor actions, torch::Tensor 
 
 void env_host_join(std::shared_ptr<Env> e) { ck(mc_env_host_join(e->h, cur_stream()), "host_join"); }
 
+void obs_to_policy(torch::Tensor obs, torch::Tensor out, int64_t layout) {
+    need(obs, "obs", at::kByte);
+    need(out, "out", at::kFloat);
+    TORCH_CHECK(obs.dim() == 4 && obs.size(3) == 3, "obs must be uint8 [B, H, W, 3]");
+    TORCH_CHECK(out.numel() == obs.numel(), "out must have as many elements as obs");
+    TORCH_CHECK(out.device() == obs.device(), "obs and out must be on the same device");
+    ck(mc_obs_to_policy(obs.data_ptr<uint8_t>(), out.data_ptr<float>(), obs.size(0), (int32_t)obs.size(1),
+                        (int32_t)obs.size(2), (int32_t)layout, cur_stream()),
+       "obs_to_policy");
+}
+
 void env_render(std::shared_ptr<Env> e) { ck(mc_env_render(e->h, cur_stream()), "render"); }
 
 void env_set_regen_mode(std::shared_ptr<Env> e, int mode) { ck(mc_env_set_regen_mode(e->h, mode), "set_regen_mode"); }
@@ -724,6 +735,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("env_step_discrete", &env_step_discrete);
     m.def("env_step_host", &env_step_host);
     m.def("env_host_join", &env_host_join);
+    m.def("obs_to_policy", &obs_to_policy);
     m.def("env_render", &env_render);
     m.def("env_set_regen_mode", &env_set_regen_mode);
     m.def("env_regenerate_if", &env_regenerate_if);

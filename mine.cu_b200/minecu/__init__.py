@@ -361,6 +361,30 @@ class MineEnv:
             _C.env_render(self._env)
         return self.obs_buffer
 
+    def policy_obs(self, out: Optional[torch.Tensor] = None, layout: str = "nchw") -> torch.Tensor:
+        """The current observation as a policy takes it: float32 in [0, 1],
+        [B, 3, H, W] ("nchw", what the reference's example policy permutes
+        its input to) or [B, H, W, 3] ("nhwc").  One pass over the uint8
+        observation (obs / 255, IEEE division); for "float32" observations,
+        which already hold those values, the permuted buffer."""
+        if layout not in ("nchw", "nhwc"):
+            raise ValueError("layout must be 'nchw' or 'nhwc'")
+        B, H, W = self.batch_size, self.render_height, self.render_width
+        shape = (B, 3, H, W) if layout == "nchw" else (B, H, W, 3)
+        if self.obs_buffer.dtype == torch.float32:
+            src = self.obs_buffer.permute(0, 3, 1, 2) if layout == "nchw" else self.obs_buffer
+            if out is None:
+                return src.contiguous()
+            out.copy_(src)
+            return out
+        if out is None:
+            out = torch.empty(shape, dtype=torch.float32, device=self.device)
+        elif tuple(out.shape) != shape or out.dtype != torch.float32 or not out.is_contiguous():
+            raise ValueError(f"out must be a contiguous float32 tensor of shape {shape}")
+        with torch.cuda.device(self.device):
+            _C.obs_to_policy(self.obs_buffer, out, 0 if layout == "nchw" else 1)
+        return out
+
     def set_regen(self, mode: str) -> None:
         """Which worlds a step's dones (and reset(mask)) regenerate: "all"
         (the reference's rule: every world when any env is done or reset) or
