@@ -12,6 +12,9 @@ the flag is set anywhere, on the device, without a host synchronisation
 the whole batch.  The all-reduce is only needed when episodes can end or
 masked resets happen; a run with neither leaves `sync_regen` off.
 
+`gather` brings every rank's rewards and dones to every rank in global env
+order (one all-gather), for a single consumer of the whole batch.
+
 Actions for a rank's envs come from the global action stream with the rank's
 first env as the offset (Philox counter = (global env, step)), so the job is
 independent of the number of ranks:
@@ -78,6 +81,26 @@ class ShardedEnv:
         if self.sync_regen:
             self._sync(torch.as_tensor(self.env.do_reset).any())
         return out
+
+    def gather(self, rewards: torch.Tensor, dones: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+        """Every rank's rewards and dones of a step, in global env order, on
+        every rank (for a single consumer such as a learner): one all-gather
+        of a [2, n] float32 block per rank (rewards, dones as 0/1), each
+        padded to the largest range.  Returns (rewards float32 [N], dones
+        bool [N]) on this rank's flag device."""
+        dev = self.flag_device
+        if self.world == 1:
+            return rewards.to(dev, torch.float32), dones.to(dev).bool()
+        counts = [shard_range(self.global_batch, self.world, r)[1] for r in range(self.world)]
+        n = max(counts)
+        block = torch.zeros((2, n), dtype=torch.float32, device=dev)
+        block[0, :self.count] = rewards.reshape(-1).to(dev, torch.float32)
+        block[1, :self.count] = dones.reshape(-1).to(dev, torch.float32)
+        parts = [torch.empty_like(block) for _ in range(self.world)]
+        dist.all_gather(parts, block, group=self.group)
+        rew = torch.cat([p[0, :c] for p, c in zip(parts, counts)])
+        done = torch.cat([p[1, :c] for p, c in zip(parts, counts)]) != 0
+        return rew, done
 
     def reset(self, mask: Optional[torch.Tensor] = None):
         obs = self.env.reset(mask)

@@ -108,6 +108,46 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _gather_main(rank, world, port, out_dir, global_b):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "mine.cu_b200"))
+    import torch.distributed as dist
+    from minecu.shard import ShardedEnv, shard_range as sr
+
+    class _Env:
+        def __init__(self, n):
+            self.batch_size = n
+            self.device = torch.device("cpu")
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        start, count = sr(global_b, world, rank)
+        env = ShardedEnv(_Env(count), global_b, sync_regen=False)
+        rew = torch.arange(start, start + count, dtype=torch.float32) * 0.5
+        done = (torch.arange(start, start + count) % 3) == 0
+        g_rew, g_done = env.gather(rew, done)
+        np.savez(os.path.join(out_dir, f"gather{rank}.npz"), rew=g_rew.numpy(), done=g_done.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("global_b", [10, 7])
+def test_gather_brings_every_ranks_results_in_env_order(global_b):
+    """ShardedEnv.gather on two gloo ranks, even and uneven ranges."""
+    import torch.multiprocessing as mp
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_gather_main, args=(2, _free_port(), d, global_b), nprocs=2, start_method="spawn",
+                           join=True)
+        for r in range(2):
+            got = np.load(os.path.join(d, f"gather{r}.npz"))
+            assert np.array_equal(got["rew"], np.arange(global_b, dtype=np.float32) * 0.5)
+            assert np.array_equal(got["done"], np.arange(global_b) % 3 == 0)
+
+
 def _run_ranks(sync):
     import torch.multiprocessing as mp
     with tempfile.TemporaryDirectory() as d:
