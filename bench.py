@@ -346,6 +346,23 @@ def run_mine(args):
                "note": "the reference's published number is float32 obs on an RTX 3090 (README.md:11,50)"}
         del env32
 
+    # the other observation modes of the reference's baseline list, same shape and window
+    modes = {}
+    if f32 is not None:
+        modes["float32"] = {"value": f32["value"], "ms_per_step": f32["ms_per_step"]}
+        for mode in ("uint8_minimal", "uint8_prebasis_full"):
+            env_m = MineEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                            device=str(dev), max_steps=W["max_steps"], obs_dtype=mode, numerics="ref_fast",
+                            form="fused", look_delta=W["look_delta"])
+            env_m.reset()
+            if Wm:
+                env_m.rollout(acts_w)
+            env_m.prepare_rollout(acts_t)
+            t_m = timed(lambda: env_m.rollout(acts_t))
+            env_m.check_error()
+            modes[mode] = {"value": B * K * world / t_m, "ms_per_step": t_m / K * 1e3}
+            del env_m
+
     peak, peak_kind = load_peaks()
     achieved = bytes_per_env_step * B / (t_fused / K) / 1e9
     line = {
@@ -383,6 +400,8 @@ def run_mine(args):
     }
     if f32 is not None:
         line["float32_obs"] = f32
+    if modes:
+        line["modes"] = modes
     if policy is not None:
         line["policy_obs"] = policy
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -659,6 +678,25 @@ def run_reference(args):
     torch.cuda.synchronize()
     te = ev0.elapsed_time(ev1) / 1e3
     e2e = B * Kr / te
+    # the other observation modes, same shape and window
+    modes = {}
+    if args.workload == "peak" and not args.shape:
+        for mode in ("float32", "uint8_minimal", "uint8_prebasis_full"):
+            env_m = ref_driver.RefEnv(batch_size=B, world_size=W["world"], render_width=W["res"],
+                                      render_height=W["res"], device=str(dev), max_steps=W["max_steps"],
+                                      obs_dtype=mode, target_block=3)
+            env_m.reset()
+            for s in range(Wm):
+                env_m.step(d_btn[s], d_look[s])
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for s in range(Kr):
+                env_m.step(d_btn[Wm + s], d_look[Wm + s])
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            t_m = ev0.elapsed_time(ev1) / 1e3
+            modes[mode] = {"value": B * Kr / t_m, "ms_per_step": t_m / Kr * 1e3}
+            del env_m
     line = {
         "impl": "reference", "metric": RENDER_METRIC if args.workload == "render" else METRIC, "value": value,
         "unit": "env-steps/s", "n_gpus": 1, "steps": Kr,
@@ -672,6 +710,8 @@ def run_reference(args):
                          "sample": f"{Kr} steps of B={B}; the reference implementation is CUDA-only, so this arm "
                                    "runs its own kernels on the same B200"},
     }
+    if modes:
+        line["modes"] = modes
     print(json.dumps(line), flush=True)
 
 
