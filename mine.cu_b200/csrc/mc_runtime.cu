@@ -556,13 +556,17 @@ static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
 }
 
 static void default_fused(mc_env* e) {
-    // Small images over small worlds: one warp per env, world staged in
-    // shared memory.  Big images or big worlds: teams of 4 warps render each
-    // env together from one staged copy of its world.  The autotuner
-    // (minecu/autotune.py) refines this per configuration.
+    // Small worlds: one warp per env, world staged in shared memory.  Big
+    // worlds, or big images over too few envs to give every resident warp
+    // (SMs x 32) two envs: teams of 4 warps render each env together from
+    // one staged copy of its world.  (16^3 worlds, 64x64 images: teams take
+    // 0.166 ms/step at B=4096, where one warp per env takes 0.206; one warp
+    // per env takes 0.492 ms/step at B=16384, where teams take 0.587.)  The
+    // autotuner (minecu/autotune.py) refines this per configuration.
     const int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
     const bool aligned = (wxyz & 15) == 0 && !(((uintptr_t)e->kp.voxels) & 15);
-    const bool big = e->cfg.render_width * e->cfg.render_height >= 64 * 64 || wxyz > 8192;
+    const bool few_envs = (long long)e->cfg.batch_size < 2LL * e->num_sms * 32;
+    const bool big = (e->cfg.render_width * e->cfg.render_height >= 64 * 64 && few_envs) || wxyz > 8192;
     e->fcfg.warps_per_cta = 8;
     if (big) {
         e->fcfg.stage = (wxyz <= 32768 && aligned) ? 1 : 0;
