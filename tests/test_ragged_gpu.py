@@ -221,3 +221,41 @@ def test_ragged_rejects_invalid(cuda):
     with pytest.raises(RuntimeError, match="repeats"):
         RaggedBatch([a, a])
     del torch
+
+
+@pytest.mark.parametrize("config", [None, (8, 3, [1, 1, 1, 1], [4, 8, 8, 8], 4, [0, 1, 1, 1])],
+                         ids=["default", "teams"])
+def test_ragged_per_env_regen_equals_separate(cuda, config):
+    """Per-env regeneration (regen="per_env") through one ragged launch equals
+    the same groups stepped alone with it.  A masked reset of a third of each
+    group's envs at step 4 offsets their episodes, so envs of one group end
+    on different steps and only their own worlds regenerate; half the actions
+    break blocks, so the worlds left alone differ from the start world."""
+    import torch
+    from minecu import _C
+    from minecu.ragged import RaggedBatch
+    ra = _make(torch, cuda, GROUPS, "uint8", "ref_fast")
+    sb = _make(torch, cuda, GROUPS, "uint8", "ref_fast")
+    for e in ra + sb:
+        e.set_regen("per_env")
+    batch = RaggedBatch(ra)
+    if config is not None:
+        batch.set_launch_config(*config)
+    batch.reset()
+    for e in sb:
+        e.reset()
+    steps = 18
+    acts = torch.empty((steps, batch.total), dtype=torch.uint8, device=cuda)
+    _C.philox_actions(acts, 0, 0, 9, True)
+    for s in range(steps):
+        if s == 4:
+            for a, b in zip(ra, sb):
+                m = (torch.arange(a.batch_size, device=cuda) % 3) == 0
+                a.reset(m)
+                b.reset(m)
+        batch.step(acts[s])
+        for g, e in enumerate(sb):
+            e.step(acts[s, batch.group_slice(g)])
+        torch.cuda.synchronize()
+        _assert_same(torch, ra, sb, f"step {s}")
+    batch.check_error()
