@@ -197,6 +197,13 @@ int mc_env_get_fused_config(const mc_env* env, mc_fused_config* cfg);
 int mc_env_check_error(mc_env* env, void* stream);
 /* Bytes of dynamic shared memory the fused kernel uses per CTA. */
 int64_t mc_env_fused_smem_bytes(const mc_env* env);
+/* The launch shape mc_env_create would choose for this configuration on a
+ * GPU with num_sms SMs (voxels_aligned: the voxels start on a 16-byte
+ * boundary), and the dynamic shared memory it uses per CTA (smem_bytes may
+ * be NULL).  Needs no GPU.  No counterpart in the reference, whose launch
+ * shapes are fixed per kernel (src/kernels.cu:2457-2494). */
+int mc_default_fused_config(const mc_env_config* cfg, int32_t num_sms, int32_t voxels_aligned, mc_fused_config* out,
+                            int64_t* smem_bytes);
 
 /* ---- ragged batches: several env handles stepped by one launch ---------
  * No counterpart in the reference, which runs one world size and one
@@ -373,9 +380,9 @@ typedef struct mc_decode_buffers {
  * _fast / _prebasis / _prebasis_full / _smem (launch_step*,
  * src/kernels.cu:2497-3243): kernels only, no world regeneration.  For
  * every mode but prebasis_full, do_reset is an input and step_count is not
- * touched (their episode logic runs in Python, minecu/__init__.py:363-366,
- * 435-436); for prebasis_full the episode check and counter update run in
- * the step.  The plain form writes the decode buffers as the reference
+ * touched and may be NULL (their episode logic runs in Python,
+ * minecu/__init__.py:363-366, 435-436); for prebasis_full the episode check
+ * and counter update run in the step.  The plain form writes the decode buffers as the reference
  * does (dec must be non-NULL); the fused form keeps them in registers. */
 int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* state, const int8_t* buttons,
                       const float* look, const mc_decode_buffers* dec, int32_t form, void* stream);
@@ -399,7 +406,9 @@ int mc_raycast_break(int8_t* voxels, const float* positions, const float* yaws, 
  * (larger batches are rejected with MC_ERR_INVALID); the array (about
  * 1.5 MB) stays on every GPU that loads the library until exit.  The first
  * call on a device looks up the array's address: make it before any stream
- * capture.  Calls share the array, so calls that overlap on the GPU race. */
+ * capture; the address is kept, so cudaDeviceReset while the library is
+ * loaded is not supported.  Calls share the array, so calls that overlap on
+ * the GPU race. */
 #define MC_NOALLOC_MAX_ENVS 65536
 int mc_step_plain_noalloc(const mc_env_config* cfg, const mc_env_state* state, const int8_t* buttons,
                           const float* look, void* stream);

@@ -149,7 +149,9 @@ __global__ void k_regen(int8_t* vox, const int8_t* tmpl, int B, int wxyz, int32_
     // is clear none of them has anything to write, count or clear.
     if (!go) return;
     {
-        if ((wxyz & 15) == 0) {
+        // 16-byte stores only when every world starts on a 16-byte boundary
+        // (a voxels view may start at any byte offset)
+        if ((wxyz & 15) == 0 && ((((uintptr_t)vox) | ((uintptr_t)tmpl)) & 15) == 0) {
             const int n16 = wxyz >> 4;
             const uint4* t4 = reinterpret_cast<const uint4*>(tmpl);
             for (long long b = blockIdx.x; b < B; b += gridDim.x) {
@@ -267,7 +269,7 @@ __global__ void k_regen_masked(int8_t* vox, const int8_t* tmpl, const uint8_t* d
     if (blockIdx.x == 0 && threadIdx.x == 0) flags[MC_FLAG_ANY_DONE] = 0;
     for (long long b = blockIdx.x; b < B; b += gridDim.x) {
         if (!do_reset[b]) continue;  // the same value for every thread of the CTA
-        if ((wxyz & 15) == 0) {
+        if ((wxyz & 15) == 0 && ((((uintptr_t)vox) | ((uintptr_t)tmpl)) & 15) == 0) {
             uint4* d4 = reinterpret_cast<uint4*>(vox + b * (long long)wxyz);
             const uint4* t4 = reinterpret_cast<const uint4*>(tmpl);
             for (int k = threadIdx.x; k < (wxyz >> 4); k += blockDim.x) d4[k] = __ldg(t4 + k);
@@ -414,11 +416,14 @@ static void fill_kp(mc_kp* k, const mc_env_config* c, const mc_env_state* s) {
     }
 }
 
-static int check_state(const mc_env_config* c, const mc_env_state* s) {
+// need_count = false: the stateless steps of every mode but prebasis_full,
+// whose episode counter is the caller's and is never read or written
+static int check_state(const mc_env_config* c, const mc_env_state* s, bool need_count = true) {
     if (!s) return fail(MC_ERR_INVALID, "state is NULL");
     if (c->batch_size == 0) return MC_OK;
+    const void* cnt = (need_count || s->step_count) ? (const void*)s->step_count : (const void*)s->voxels;
     const void* req[] = {s->voxels, s->positions, s->velocities, s->yaws, s->pitches, s->on_ground,
-                         s->step_count, s->do_reset, s->cameras, s->obs, s->rewards};
+                         cnt, s->do_reset, s->cameras, s->obs, s->rewards};
     const char* names[] = {"voxels", "positions", "velocities", "yaws", "pitches", "on_ground",
                            "step_count", "do_reset", "cameras", "obs", "rewards"};
     for (int i = 0; i < 11; ++i)
@@ -535,9 +540,10 @@ int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* t
 
 static bool team_mode(const mc_fused_cfg& f) { return f.team_warps > 1 || f.coop; }
 
-static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
+static int validate_fused_kp(const mc_env_config* cfg, const mc_kp* kp, const mc_backend* be,
+                             const mc_fused_cfg* f) {
     if (team_mode(*f)) {
-        const mc_kp* kps[1] = {&e->kp};
+        const mc_kp* kps[1] = {kp};
         return team_validate(kps, 1, &f->stage, &f->tile_w, &f->coop, f->team_warps, f->warps_per_cta,
                              f->ctas_per_sm);
     }
@@ -547,43 +553,88 @@ static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
     if (f->tile_w != 4 && f->tile_w != 8 && f->tile_w != 16 && f->tile_w != 32)
         return fail(MC_ERR_INVALID, "tile_w must be 4, 8, 16 or 32");
     if (f->ctas_per_sm < 1 || f->ctas_per_sm > 32) return fail(MC_ERR_INVALID, "ctas_per_sm out of range");
-    int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
+    int wxyz = cfg->world_x * cfg->world_y * cfg->world_z;
     if (f->stage && (wxyz & 15)) return fail(MC_ERR_INVALID, "stage needs world bytes %% 16 == 0");
-    mc_kp k = e->kp;
-    size_t smem = e->be->fused_smem_bytes(&k, f);
+    mc_kp k = *kp;
+    size_t smem = be->fused_smem_bytes(&k, f);
     if (smem > 227 * 1024) return fail(MC_ERR_INVALID, "fused shared memory %zu > 227 KB", smem);
     return MC_OK;
 }
 
-static void default_fused(mc_env* e) {
-    // Small worlds: one warp per env, world staged in shared memory.  Big
-    // worlds, or big images over too few envs to give every resident warp
-    // (SMs x 32) two envs: teams of 4 warps render each env together from
-    // one staged copy of its world.  (16^3 worlds, 64x64 images: teams take
-    // 0.166 ms/step at B=4096, where one warp per env takes 0.206; one warp
-    // per env takes 0.492 ms/step at B=16384, where teams take 0.587.)  The
-    // autotuner (minecu/autotune.py) refines this per configuration.
-    const int wxyz = e->cfg.world_x * e->cfg.world_y * e->cfg.world_z;
-    const bool aligned = (wxyz & 15) == 0 && !(((uintptr_t)e->kp.voxels) & 15);
-    const bool few_envs = (long long)e->cfg.batch_size < 2LL * e->num_sms * 32;
-    const bool big = (e->cfg.render_width * e->cfg.render_height >= 64 * 64 && few_envs) || wxyz > 8192;
-    e->fcfg.warps_per_cta = 8;
+static int validate_fused(const mc_env* e, const mc_fused_cfg* f) {
+    return validate_fused_kp(&e->cfg, &e->kp, e->be, f);
+}
+
+// The default launch shape of an env (a pure function of its configuration,
+// the voxels' alignment and the SM count).  Small worlds: one warp per env,
+// world staged in shared memory.  Big worlds, or big images over too few
+// envs to give every resident warp (SMs x 32) two envs: teams of 4 warps
+// render each env together from one staged copy of its world.  (16^3
+// worlds, 64x64 images: teams take 0.166 ms/step at B=4096, where one warp
+// per env takes 0.206; one warp per env takes 0.492 ms/step at B=16384,
+// where teams take 0.587.)  A shape whose shared memory does not fit falls
+// back to the team shape (whose per-warp image band is half as tall), then
+// to one team per CTA, then to unstaged worlds.  The autotuner (minecu/autotune.py) refines the
+// shape per configuration.
+static mc_fused_cfg default_launch(const mc_env_config* cfg, const mc_kp* kp, const mc_backend* be, int num_sms) {
+    const int wxyz = cfg->world_x * cfg->world_y * cfg->world_z;
+    const bool aligned = (wxyz & 15) == 0 && !(((uintptr_t)kp->voxels) & 15);
+    const bool few_envs = (long long)cfg->batch_size < 2LL * num_sms * 32;
+    const bool big = (cfg->render_width * cfg->render_height >= 64 * 64 && few_envs) || wxyz > 8192;
+    auto team_shape = [&](mc_fused_cfg& f) {
+        f.warps_per_cta = 8;
+        f.stage = (wxyz <= 32768 && aligned) ? 1 : 0;
+        f.ctas_per_sm = 3;
+        f.tile_w = 8;
+        f.team_warps = 4;
+        f.coop = 1;
+    };
+    mc_fused_cfg f;
     if (big) {
-        e->fcfg.stage = (wxyz <= 32768 && aligned) ? 1 : 0;
-        e->fcfg.ctas_per_sm = 3;
-        e->fcfg.tile_w = 8;
-        e->fcfg.team_warps = 4;
-        e->fcfg.coop = 1;
+        team_shape(f);
     } else {
-        e->fcfg.stage = (wxyz <= 8192 && aligned) ? 1 : 0;
-        e->fcfg.ctas_per_sm = 4;
-        e->fcfg.tile_w = 4;
-        e->fcfg.team_warps = 1;
-        e->fcfg.coop = 0;
+        f.warps_per_cta = 8;
+        f.stage = (wxyz <= 8192 && aligned) ? 1 : 0;
+        f.ctas_per_sm = 4;
+        f.tile_w = 4;
+        f.team_warps = 1;
+        f.coop = 0;
     }
-    if (validate_fused(e, &e->fcfg) != MC_OK) {  // e.g. a world too big for one team's shared memory
-        e->fcfg.stage = 0;
+    const std::string saved = mc_last_error();  // probing shapes must not replace the caller's message
+    if (!big && validate_fused_kp(cfg, kp, be, &f) != MC_OK) team_shape(f);  // e.g. wide float32 images
+    if (validate_fused_kp(cfg, kp, be, &f) != MC_OK) f.warps_per_cta = 4;    // one team per CTA
+    if (validate_fused_kp(cfg, kp, be, &f) != MC_OK) f.stage = 0;  // e.g. a world too big for a team's copy
+    mc_set_error(MC_OK, saved.c_str());
+    return f;
+}
+
+static void default_fused(mc_env* e) { e->fcfg = default_launch(&e->cfg, &e->kp, e->be, e->num_sms); }
+
+extern "C" int mc_default_fused_config(const mc_env_config* cfg, int32_t num_sms, int32_t voxels_aligned,
+                                       mc_fused_config* out, int64_t* smem_bytes) {
+    if (!out) return fail(MC_ERR_INVALID, "out is NULL");
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    if (num_sms < 1) return fail(MC_ERR_INVALID, "num_sms must be >= 1");
+    mc_kp k;
+    fill_kp(&k, cfg, nullptr);
+    k.voxels = voxels_aligned ? nullptr : reinterpret_cast<int8_t*>((uintptr_t)1);
+    const mc_backend* be = backend_of(cfg->numerics);
+    mc_fused_cfg f = default_launch(cfg, &k, be, num_sms);
+    rc = validate_fused_kp(cfg, &k, be, &f);
+    if (rc) return rc;
+    *out = mc_fused_config{f.stage, f.warps_per_cta, f.ctas_per_sm, f.tile_w, f.team_warps, f.coop};
+    if (smem_bytes) {
+        if (team_mode(f)) {
+            const mc_kp* kps[1] = {&k};
+            mc_ragged_kp rk;
+            team_layout(kps, 1, &f.stage, &f.tile_w, &f.coop, f.team_warps, f.warps_per_cta, &rk);
+            *smem_bytes = team_smem(rk, f.warps_per_cta);
+        } else {
+            *smem_bytes = (int64_t)be->fused_smem_bytes(&k, &f);
+        }
     }
+    return MC_OK;
 }
 
 static void drop_graphs(mc_env* e) {
@@ -1475,7 +1526,7 @@ extern "C" int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* s
                                  const float* look, const mc_decode_buffers* dec, int32_t form, void* stream) {
     int rc = check_config(cfg);
     if (rc) return rc;
-    rc = check_state(cfg, st);
+    rc = check_state(cfg, st, cfg->obs_mode == MC_OBS_UINT8_PREBASIS_FULL);
     if (rc) return rc;
     if (cfg->batch_size == 0) return MC_OK;
     if (!buttons || !look) return fail(MC_ERR_INVALID, "buttons/look are NULL");
@@ -1686,7 +1737,7 @@ int mc_step_stateless_with_flags(const mc_env_config* cfg, const mc_env_state* s
                                  void* stream) {
     int rc = check_config(cfg);
     if (rc) return rc;
-    rc = check_state(cfg, st);
+    rc = check_state(cfg, st, cfg->obs_mode == MC_OBS_UINT8_PREBASIS_FULL);
     if (rc) return rc;
     if (cfg->batch_size == 0) return MC_OK;
     if (!buttons || !look) return fail(MC_ERR_INVALID, "buttons/look are NULL");

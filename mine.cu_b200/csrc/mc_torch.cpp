@@ -152,14 +152,11 @@ void run_step(const StepTensors& T, int obs_mode, torch::Tensor* basis, torch::T
     s.cameras = ptr<float>(T.cameras);
     s.obs = T.obs_buffer.data_ptr();
     s.rewards = ptr<float>(T.rewards);
-    torch::Tensor dummy_cnt;
     if (step_count) {
         need(*step_count, "step_count", at::kInt);
+        need_shape(*step_count, "step_count", {T.voxels.size(0)});
         s.step_count = ptr<int32_t>(*step_count);
-    } else {
-        dummy_cnt = torch::zeros({T.voxels.size(0)}, T.voxels.options().dtype(at::kInt));
-        s.step_count = ptr<int32_t>(dummy_cnt);
-    }
+    }  // else NULL: these modes' episode counter lives in Python and the step never touches it
     if (basis) {
         need(*basis, "basis", at::kFloat);
         need_shape(*basis, "basis", {T.voxels.size(0), 14});

@@ -121,6 +121,7 @@ _PROTOS = {
     "mc_env_get_fused_config": (I, [P, ctypes.POINTER(FusedConfig)]),
     "mc_env_check_error": (I, [P, P]),
     "mc_env_fused_smem_bytes": (ctypes.c_int64, [P]),
+    "mc_default_fused_config": (I, [PCFG, c_int32, c_int32, P, P]),
     "mc_ragged_create": (I, [ctypes.POINTER(c_void_p), I, ctypes.POINTER(c_void_p)]),
     "mc_ragged_destroy": (I, [P]),
     "mc_ragged_set_config": (I, [P, ctypes.POINTER(RaggedConfig)]),

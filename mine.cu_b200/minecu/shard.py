@@ -66,10 +66,23 @@ class ShardedEnv:
             raise ValueError(f"rank {self.rank} holds envs [{self.start}, {self.start + self.count}); "
                              f"its env has batch_size {n}")
         self.global_batch = global_batch
-        # per-env regeneration couples no envs: nothing to all-reduce
-        self.sync_regen = sync_regen and self.world > 1 and getattr(env, "regen", "all") == "all"
+        self._sync_requested = sync_regen and self.world > 1
         self.flag_device = flag_device if flag_device is not None else getattr(env, "device", torch.device("cpu"))
         self._flag = torch.zeros(1, dtype=torch.uint8, device=self.flag_device)
+
+    @property
+    def sync_regen(self) -> bool:
+        """Whether a step or reset all-reduces the any-done flag: asked for,
+        more than one rank, and the env's regeneration rule is "all" (read at
+        every step, so `env.set_regen` after construction takes effect; per-env
+        regeneration couples no envs and needs nothing)."""
+        return self._sync_requested and getattr(self.env, "regen", "all") == "all"
+
+    def set_regen(self, mode: str) -> None:
+        """Switch the env's regeneration rule ("all" or "per_env").  Every
+        rank must make the same switch between the same two steps, since the
+        all-reduce runs on every rank or on none."""
+        self.env.set_regen(mode)
 
     def _sync(self, local_any: torch.Tensor) -> None:
         self._flag.copy_(local_any.reshape(1).to(device=self.flag_device, dtype=torch.uint8))

@@ -99,3 +99,40 @@ def test_server_admission_arithmetic_and_config_checks():
     assert L.mc_server_create(ctypes.byref(bad), ctypes.byref(out)) == capi.MC_ERR_INVALID
     assert "max_inflight" in capi.last_error()
     assert L.mc_server_destroy(None) == capi.MC_OK
+
+
+def _default_shape(B, W, H, world, obs_dtype, sms=148, aligned=1):
+    L = capi.lib()
+    c = capi.make_config(B, world, world, world, W, H, obs_dtype=obs_dtype)
+    f = capi.FusedConfig()
+    smem = ctypes.c_int64(-1)
+    rc = L.mc_default_fused_config(ctypes.byref(c), sms, aligned, ctypes.byref(f), ctypes.byref(smem))
+    assert rc == capi.MC_OK, capi.last_error()
+    return f, smem.value
+
+
+@pytest.mark.parametrize("B,W,H,world,mode", [
+    (32768, 32, 32, 16, "uint8"), (4096, 64, 64, 32, "uint8"), (9472, 64, 64, 16, "uint8"),
+    (9472, 320, 320, 16, "float32"), (9472, 1280, 8, 16, "uint8"), (4096, 320, 320, 16, "float32"),
+    (20000, 512, 512, 16, "float32"), (2048, 1024, 1024, 16, "float32"), (64, 7, 5, 8, "uint8_minimal"),
+    (100, 16, 16, 64, "uint8"),
+])
+def test_default_launch_shape_fits_shared_memory(B, W, H, world, mode):
+    """The default shape of every configuration validates (mc_env_create
+    launches it unchanged), including wide float32 images at batches that
+    pick one warp per env, whose image band alone can exceed 227 KB."""
+    f, smem = _default_shape(B, W, H, world, mode)
+    assert 0 < smem <= 227 * 1024, (f.stage, f.warps_per_cta, f.team_warps, f.coop, smem)
+
+
+def test_default_launch_shape_choices():
+    f, _ = _default_shape(32768, 32, 32, 16, "uint8")
+    assert (f.stage, f.team_warps, f.coop, f.tile_w) == (1, 1, 0, 4)  # one warp per env, staged
+    f, _ = _default_shape(4096, 64, 64, 32, "uint8")
+    assert (f.stage, f.team_warps, f.coop) == (1, 4, 1)  # teams over staged 32 KB worlds
+    f, _ = _default_shape(9472, 64, 64, 16, "uint8")
+    assert (f.team_warps, f.coop) == (1, 0)  # two envs per resident warp: one warp per env
+    f, _ = _default_shape(9472, 320, 320, 16, "float32")
+    assert f.coop == 1  # the one-warp band does not fit: team shape
+    f, _ = _default_shape(32768, 32, 32, 16, "uint8", aligned=0)
+    assert f.stage == 0  # bulk copies need 16-byte aligned worlds

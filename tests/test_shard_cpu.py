@@ -44,6 +44,10 @@ class _OracleShard:
                              episode_length=EPISODE)
         self.batch_size = n
         self.device = torch.device("cpu")
+        self.regen = "all"  # the oracle env applies the all-world rule; ShardedEnv reads this mode
+
+    def set_regen(self, mode):
+        self.regen = mode
 
     @property
     def do_reset(self):
@@ -83,7 +87,7 @@ def _trajectory(env, start, count, sharded):
     return {k: np.stack(v) for k, v in out.items()}
 
 
-def _rank_main(rank, world, port, out_dir, sync):
+def _rank_main(rank, world, port, out_dir, sync, switch=False):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     for sub in ("mine.cu_b200", "oracle", "tests"):
@@ -95,7 +99,14 @@ def _rank_main(rank, world, port, out_dir, sync):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         start, count = sr(GLOBAL_B, world, rank)
-        env = ShardedEnv(_OracleShard(count), GLOBAL_B, sync_regen=sync)
+        inner = _OracleShard(count)
+        if switch:
+            inner.regen = "per_env"  # built under the per-env rule, switched before the first step
+        env = ShardedEnv(inner, GLOBAL_B, sync_regen=sync)
+        if switch:
+            assert not env.sync_regen
+            env.set_regen("all")
+            assert env.sync_regen
         traj = _trajectory(env, start, count, True)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), start=start, **traj)
     finally:
@@ -148,10 +159,11 @@ def test_gather_brings_every_ranks_results_in_env_order(global_b):
             assert np.array_equal(got["done"], np.arange(global_b) % 3 == 0)
 
 
-def _run_ranks(sync):
+def _run_ranks(sync, switch=False):
     import torch.multiprocessing as mp
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_rank_main, args=(2, _free_port(), d, sync), nprocs=2, start_method="spawn", join=True)
+        mp.start_processes(_rank_main, args=(2, _free_port(), d, sync, switch), nprocs=2, start_method="spawn",
+                           join=True)
         parts = [dict(np.load(os.path.join(d, f"rank{r}.npz"))) for r in range(2)]
     return {k: np.concatenate([p[k] for p in parts], axis=1) for k in parts[0] if k != "start"}
 
@@ -173,3 +185,14 @@ def test_two_ranks_without_sync_drift_apart():
     whole = _trajectory(_OracleShard(GLOBAL_B), 0, GLOBAL_B, False)
     split = _run_ranks(sync=False)
     assert not np.array_equal(whole["voxels"], split["voxels"])
+
+
+@pytest.mark.timeout(300)
+def test_regen_mode_switched_after_construction_takes_effect():
+    """A ShardedEnv built while its env regenerates per env, then switched to
+    the all-world rule with set_regen, all-reduces the any-done flag from
+    the next step on: the ranks again equal one env holding the batch."""
+    whole = _trajectory(_OracleShard(GLOBAL_B), 0, GLOBAL_B, False)
+    split = _run_ranks(sync=True, switch=True)
+    for k in whole:
+        assert np.array_equal(whole[k], split[k]), k
