@@ -184,6 +184,14 @@ int mc_env_regenerate_if(mc_env* env, const uint8_t* flag, void* stream);
 int mc_env_set_regen_mode(mc_env* env, int32_t mode);
 /* The mode, or a negative status. */
 int mc_env_get_regen_mode(const mc_env* env);
+/* Budget of the fused kernels' bounded waits for a bulk copy of a world into
+ * shared memory: polls > 0 polls, 0 = give up at once (makes every wait run
+ * out, to test the timeout path), < 0 = the default (2^22 polls).  A wait
+ * that runs out records a timeout in the error word (mc_env_check_error)
+ * and the warp renders that env and every later one from global memory, so
+ * the results stay the same.  No counterpart in the reference, which has no
+ * bulk copies. */
+int mc_env_set_wait_limit(mc_env* env, int32_t polls);
 /* K fused steps of discrete actions actions[K,B] captured once in a CUDA
  * graph and replayed; rewards_out / dones_out ([K,B], optional) receive each
  * step's rewards and dones.  The graph is cached per (actions, outputs, K). */

@@ -1467,9 +1467,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Bounded wait on an mbarrier phase; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (int it = 0; it < (1 << 22); ++it) {
+// Bounded wait on an mbarrier phase; returns false on timeout.  polls: 0 =
+// MC_WAIT_POLLS_DEFAULT, n > 0 = n polls, < 0 = none (the timeout path's test).
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int polls = 0) {
+    const int limit = polls == 0 ? MC_WAIT_POLLS_DEFAULT : (polls < 0 ? 0 : polls);
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -1576,13 +1578,14 @@ __device__ __forceinline__ RayPar ray_par(const mc_kp& p) {
 }
 
 // One pixel's ray through one of the two voxel sources.
-template <int FAM, class V>
+// VDLIM = false: view-limited worlds take the reference-shaped loop (fewer registers).
+template <int FAM, class V, bool VDLIM = true>
 __device__ __forceinline__ Hit march_pixel(const RayPar& p, const Cam& c, const Dda0& d0, float u, float v,
                                            const V& vox, bool inside, bool skip_first, bool sky_exit = false,
                                            bool vd_safe = false, int ytop = 1 << 20) {
     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST)
-        return shade_ray<FAM == MC_FAM_SHADED_FAST>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd, p.gh,
-                                                    inside, skip_first, sky_exit, vd_safe, ytop);
+        return shade_ray<FAM == MC_FAM_SHADED_FAST, V, VDLIM>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, p.vd,
+                                                              p.gh, inside, skip_first, sky_exit, vd_safe, ytop);
     if (FAM == MC_FAM_FP16) return fp16_ray(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     return flat_ray<FAM != MC_FAM_PREBASIS>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit,
                                               ytop);
@@ -1633,11 +1636,23 @@ __device__ __forceinline__ int staged_top_layer(const int8_t* world, int wx, int
 // same kernel needed spill slots at its 64-register budget (4 CTAs of 8 warps
 // per SM) and ran 8% slower on B=32768, 16^3, 32x32, so it keeps its own
 // copy; the parity tests hold the two kernels to the same bits.
+// Per-env facts of a render (EnvRender::bits).
+enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
+
+// The rest of a per-warp launch for a warp whose bulk copy timed out
+// (defined after render_env): env e, already stepped, and every env the
+// warp claims after it, rendered from the worlds in global memory.  Called
+// after the main loop and out of line, so the staged path keeps its
+// registers.  Returns whether any of those envs was done.
+template <int FAM, bool F32>
+__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long total_warps,
+                                                      int tile_w, int lane, FusedCtx cx);
+
 #ifndef MC_FUSED_MIN_BLOCKS
 #define MC_FUSED_MIN_BLOCKS 4
 #endif
 template <int FAM, bool F32, bool STAGE>
-__global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p, int tile_w) {
+__global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const __grid_constant__ mc_kp p, int tile_w) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -1688,13 +1703,16 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
     __syncthreads();
     uint32_t phase = 0;
     bool any_done = false;
-    bool failed = false;
+    bool no_stage = false;        // a copy timed out: this warp renders from global memory from now on
+    bool pending = false;         // ... and that copy may still be in flight
+    uint32_t pending_phase = 0;   // its phase, waited for before the warp leaves
     const float rcp_vd = N::rcp_of(p.vd);
 
     const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
     const long long total_warps = (long long)gridDim.x * nwarps;
     const long long first = p.sched_dynamic ? next_env(p, 0, total_warps, lane) : (long long)blockIdx.x * nwarps + warp;
-    for (long long e = first; e < p.B && !failed; e = next_env(p, e, total_warps, lane)) {
+    long long e = first;
+    for (; e < p.B; e = next_env(p, e, total_warps, lane)) {
         // ---- agent step (every lane computes the same values) --------------
         int8_t btn[8];
         float l0, l1;
@@ -1835,13 +1853,14 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
                     "l"(gw), "r"(wxyz), "r"(mbar_a)
                     : "memory");
             }
-            bool ok = mbar_wait(mbar_a, phase);
-            phase ^= 1u;
-            if (!ok) {
+            if (!mbar_wait(mbar_a, phase, p.wait_polls)) {
                 if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
-                failed = true;
-                break;
+                no_stage = true;  // the copy may still land in this warp's buffer: never read it again
+                pending = true;
+                pending_phase = phase;
+                break;            // env e and the rest: fused_finish_from_global below
             }
+            phase ^= 1u;
             // the interaction may have written after the copy read the byte
             if (lane == 0 && mod_idx >= 0) sworld[mod_idx] = mod_val;
             __syncwarp();
@@ -1925,6 +1944,21 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(mc_kp p
             __syncwarp();
         }
     }
+    if (STAGE && no_stage) {
+        FusedCtx cx;
+        cx.s_u = s_u;
+        cx.s_v = s_v;
+        cx.s_rgb = s_rgb;
+        cx.s_sky = s_sky;
+        cx.s_rgb8 = s_rgb8;
+        cx.s_sky8 = s_sky8;
+        cx.stage = stage;
+        cx.rcp_vd = rcp_vd;
+        any_done |= fused_finish_from_global<FAM, F32>(p, e, total_warps, tile_w, lane, cx);
+        // the timed-out copy may still be in flight: let it land (bounded, with
+        // the default budget) before this warp's part of shared memory can be released
+        if (pending) mbar_wait(mbar_a, pending_phase);
+    }
     // No CTA barrier here: warps leave as soon as their last env is done.
     if (lane == 0) {
         if (any_done) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
@@ -1968,8 +2002,6 @@ struct EnvRender {
     int ytop;      // no solid voxel above this layer (wy - 1 unless measured)
 };
 
-
-enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
 
 struct TeamShared {
     unsigned unit[2];  // claimed units, alternating slots
@@ -2132,7 +2164,7 @@ __device__ __forceinline__ void fill_env(const mc_kp& p, long long e, const EnvR
 
 // March row bands of env e's image with one warp: every band when band_ctr is
 // null, else the bands this warp claims from the team's shared counter.
-template <int FAM, bool F32, class V>
+template <int FAM, bool F32, class V, bool VDLIM = true>
 __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const EnvRender& r, const FusedCtx& cx,
                                            const V& vox, int tile_w, int lane, int* band_ctr) {
     // parameters in registers: p may live in shared memory, which the band
@@ -2169,7 +2201,8 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
             const int px = tx0 + lx;
             if (px < W && py < H) {
                 const float u = cx.s_u[px];
-                Hit h = march_pixel<FAM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe, r.ytop);
+                Hit h = march_pixel<FAM, V, VDLIM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe,
+                                                   r.ytop);
                 const int so = ly * W + px;  // pixel within the staged band
                 if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                     float rgb[3];
@@ -2211,9 +2244,56 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
     }
 }
 
+template <int FAM, bool F32>
+__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long total_warps,
+                                                      int tile_w, int lane, FusedCtx cx) {
+    const long long wxyz = (long long)p.wx * p.wy * p.wz;
+    if (e < p.B) {
+        // env e was stepped and found not buried: its camera, as stored by the
+        // step, gives the same render constants bit for bit
+        EnvRender r;
+        const float* cam = p.cameras + e * 5;
+        __syncwarp();
+        if (FAM == MC_FAM_PREBASIS) {
+            float bas[13];
+            basis_compute(cam[0], cam[1], cam[2], cam[3], cam[4], p.W, p.H, p.fov, bas);
+            r.c = cam_from_basis(bas);
+        } else {
+            r.c = cam_trig(cam[0], cam[1], cam[2], cam[3], cam[4]);
+        }
+        const int ey = (int)floorf(r.c.eye_y);
+        bool inside = false, skip_first;
+        if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
+            inside = eye_inside(r.c, p.wx, p.wy, p.wz, p.vd);
+            skip_first = inside && p.vd > 0.0f && p.max_steps > 0 && !(FAM == MC_FAM_SHADED_FAST && ey < p.gh);
+        } else {
+            skip_first = p.max_steps > 0;  // not buried: the eye's voxel holds air or lies outside the world
+        }
+        r.bits = (inside ? MC_ER_INSIDE : 0) | (skip_first ? MC_ER_SKIP : 0);
+        r.fill_blk = AIR;
+        r.mod_idx = -1;
+        r.mod_val = 0;
+        r.ytop = p.wy - 1;
+        render_env<FAM, F32, VoxGlobal, false>(p, e, r, cx, VoxGlobal{p.voxels + e * wxyz}, tile_w, lane, nullptr);
+        e = next_env(p, e, total_warps, lane);
+    }
+    bool any_done = false;
+    const ActionSrc act{p.actions, p.buttons, p.look};
+    for (; e < p.B; e = next_env(p, e, total_warps, lane)) {
+        EnvRender r = agent_step<FAM>(p, act, e, lane);
+        any_done |= (r.bits & MC_ER_DONE) != 0;
+        if (r.bits & MC_ER_BURIED)
+            fill_env<FAM, F32>(p, e, r, cx, lane, 32);
+        else
+            render_env<FAM, F32, VoxGlobal, false>(p, e, r, cx, VoxGlobal{p.voxels + e * wxyz}, tile_w, lane,
+                                                   nullptr);
+    }
+    return any_done;
+}
+
 // Bulk copy of one world into shared memory, waited for with a bound.
 __device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, int8_t* dst, const int8_t* src,
-                                            int bytes, int lane) {
+                                            int bytes, int lane, int polls) {
     if (lane == 0) {
         // generic-proxy reads of the previous world must precede the copy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -2224,7 +2304,7 @@ __device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, in
             "l"(src), "r"(bytes), "r"(mbar_a)
             : "memory");
     }
-    const bool ok = mbar_wait(mbar_a, phase);
+    const bool ok = mbar_wait(mbar_a, phase, polls);
     phase ^= 1u;
     return ok;
 }
@@ -2276,7 +2356,8 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     const int bar = 1 + team, nthr = TWN * 32;
     uint32_t phase = 0;
     unsigned done_groups = 0;
-    bool warp_no_stage = false;
+    bool warp_no_stage = false;   // a copy of this warp timed out: it renders from global memory from now on
+    uint32_t pending_phase = 0;   // that copy's phase, waited for before the warp leaves
     for (int k = 0;; ++k) {
         const unsigned u = ts->unit[k & 1];
         if (u >= total_units) break;
@@ -2312,7 +2393,8 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
             }
             staged = ((rk.stage_mask >> g) & 1) && !(r.bits & MC_ER_BURIED) && !warp_no_stage;
             if (staged) {
-                if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane)) {
+                const uint32_t ph = phase;
+                if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane, p.wait_polls)) {
                     // the interaction may have written after the copy read the byte
                     if (lane == 0 && r.mod_idx >= 0) world[r.mod_idx] = (int8_t)r.mod_val;
                     __syncwarp();
@@ -2320,6 +2402,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                 } else {
                     if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
                     warp_no_stage = true;  // the copy may still land: render from global memory from now on
+                    pending_phase = ph;
                     staged = false;
                 }
             }
@@ -2345,6 +2428,9 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
         if (claimer) ts->unit[(k + 1) & 1] = claim(k + 1);
         team_sync(bar, nthr);
     }
+    // a timed-out copy may still be in flight: let it land (bounded) before
+    // this warp's part of shared memory can be released
+    if (warp_no_stage) mbar_wait(cx.mbar_a, pending_phase);
     if (lane == 0) {
         for (int g = 0; g < G; ++g)
             if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);

@@ -12,6 +12,16 @@
 
 #define MC_HIDDEN __attribute__((visibility("hidden")))
 
+// NVTX range over a host phase (header-only NVTX3: a no-op unless a
+// profiler that collects NVTX is attached).
+#include <nvtx3/nvToolsExt.h>
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 struct RolloutGraph {
     cudaGraphExec_t exec = nullptr;
     const uint8_t* actions = nullptr;

@@ -26,6 +26,10 @@ enum {
 // Error codes a kernel can record in flags[MC_FLAG_ERROR] (never a trap).
 enum { MC_KERR_NONE = 0, MC_KERR_TMA_TIMEOUT = 1 };
 
+// Polls of an mbarrier before a bulk-copy wait gives up (each poll is one
+// try_wait, which itself blocks for a short hardware-defined time).
+#define MC_WAIT_POLLS_DEFAULT (1 << 22)
+
 // Everything one step launch needs, passed to kernels by value.
 struct mc_kp {
     // sizes
@@ -47,6 +51,8 @@ struct mc_kp {
     int obs_f32;  // float32 obs (else uint8)
     float look_delta;  // discrete-action look step (radians)
     int regen_per_env; // MC_REGEN_PER_ENV: a done (or reset) env regenerates only its own world
+    int wait_polls;    // bounded waits on a bulk copy: 0 = MC_WAIT_POLLS_DEFAULT polls, n > 0 = n polls,
+                       // < 0 = give up at once (a test of the timeout path)
     // state (device, borrowed from the caller)
     int8_t* voxels;
     float* positions;

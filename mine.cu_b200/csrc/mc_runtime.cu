@@ -735,9 +735,11 @@ extern "C" int mc_env_set_state(mc_env* e, const mc_env_state* s) {
     e->st = *s;
     int32_t* flags = e->kp.flags;
     const int8_t* tmpl = e->kp.world_template;
+    const int polls = e->kp.wait_polls;
     fill_kp(&e->kp, &e->cfg, s);
     e->kp.flags = flags;
     e->kp.world_template = tmpl;
+    e->kp.wait_polls = polls;
     e->kp.regen_per_env = e->regen_mode == MC_REGEN_PER_ENV;
     e->kp.sched_dynamic = 1;
     drop_graphs(e);
@@ -777,6 +779,7 @@ static int render_obs(mc_env* e, cudaStream_t s) {
 }
 
 extern "C" int mc_env_reset(mc_env* e, const uint8_t* mask, void* stream) {
+    NvtxRange nvtx("mc_env_reset");
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     cudaStream_t s = (cudaStream_t)stream;
     if (e->cfg.batch_size == 0) return MC_OK;
@@ -825,6 +828,7 @@ static int do_step(mc_env* e, const int8_t* buttons, const float* look, const ui
 }
 
 extern "C" int mc_env_step(mc_env* e, const int8_t* buttons, const float* look, int form, void* stream) {
+    NvtxRange nvtx("mc_env_step");
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     if (e->cfg.batch_size && (!buttons || !look)) return fail(MC_ERR_INVALID, "buttons/look are NULL");
     if (((uintptr_t)look) & 3) return fail(MC_ERR_INVALID, "look must be 4-byte aligned");
@@ -832,6 +836,7 @@ extern "C" int mc_env_step(mc_env* e, const int8_t* buttons, const float* look, 
 }
 
 extern "C" int mc_env_step_discrete(mc_env* e, const uint8_t* actions, int form, void* stream) {
+    NvtxRange nvtx("mc_env_step_discrete");
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     if (e->cfg.batch_size && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
     return do_step(e, nullptr, nullptr, actions, form, (cudaStream_t)stream);
@@ -902,6 +907,7 @@ static int hostio_join(const HostIO* h, cudaStream_t s) {
 
 extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* host_rewards, uint8_t* host_dones,
                                 int form, void* stream) {
+    NvtxRange nvtx("mc_env_step_host");
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     const long long B = e->cfg.batch_size;
     if (B == 0) return MC_OK;
@@ -939,6 +945,13 @@ extern "C" int mc_env_set_regen_mode(mc_env* e, int32_t mode) {
     return MC_OK;
 }
 
+extern "C" int mc_env_set_wait_limit(mc_env* e, int32_t polls) {
+    if (!e) return fail(MC_ERR_INVALID, "env is NULL");
+    e->kp.wait_polls = polls < 0 ? 0 : (polls == 0 ? -1 : polls);
+    drop_graphs(e);  // captured steps hold the old budget
+    return MC_OK;
+}
+
 extern "C" int mc_env_get_regen_mode(const mc_env* e) {
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     return e->regen_mode;
@@ -952,6 +965,7 @@ extern "C" int mc_env_regenerate_if(mc_env* e, const uint8_t* flag, void* stream
 }
 
 extern "C" int mc_env_render(mc_env* e, void* stream) {
+    NvtxRange nvtx("mc_env_render");
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     return render_obs(e, (cudaStream_t)stream);
 }
@@ -1031,6 +1045,7 @@ extern "C" int mc_env_rollout_prepare(mc_env* e, const uint8_t* actions, int32_t
 
 extern "C" int mc_env_rollout(mc_env* e, const uint8_t* actions, int32_t K, float* rewards_out, uint8_t* dones_out,
                               void* stream) {
+    NvtxRange nvtx("mc_env_rollout");
     int rc = rollout_args(e, actions, K);
     if (rc || K == 0 || e->cfg.batch_size == 0) return rc;
     RolloutGraph* g;
@@ -1289,6 +1304,7 @@ static int ragged_do_step(mc_ragged* r, const int8_t* buttons, const float* look
 }
 
 extern "C" int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* look, void* stream) {
+    NvtxRange nvtx("mc_ragged_step");
     if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
     if (mc_ragged_total_envs(r) > 0 && (!buttons || !look)) return fail(MC_ERR_INVALID, "buttons/look are NULL");
     if (((uintptr_t)look) & 3) return fail(MC_ERR_INVALID, "look must be 4-byte aligned");
@@ -1296,6 +1312,7 @@ extern "C" int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* 
 }
 
 extern "C" int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, void* stream) {
+    NvtxRange nvtx("mc_ragged_step_discrete");
     if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
     if (mc_ragged_total_envs(r) > 0 && !actions) return fail(MC_ERR_INVALID, "actions is NULL");
     return ragged_do_step(r, nullptr, nullptr, actions, (cudaStream_t)stream, false);
@@ -1303,6 +1320,7 @@ extern "C" int mc_ragged_step_discrete(mc_ragged* r, const uint8_t* actions, voi
 
 extern "C" int mc_ragged_step_host(mc_ragged* r, const uint8_t* host_actions, float* host_rewards,
                                    uint8_t* host_dones, void* stream) {
+    NvtxRange nvtx("mc_ragged_step_host");
     if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
     const long long B = mc_ragged_total_envs(r);
     if (B == 0) return MC_OK;
@@ -1375,6 +1393,7 @@ extern "C" int mc_ragged_rollout_prepare(mc_ragged* r, const uint8_t* actions, i
 }
 
 extern "C" int mc_ragged_rollout(mc_ragged* r, const uint8_t* actions, int32_t K, void* stream) {
+    NvtxRange nvtx("mc_ragged_rollout");
     if (!r) return fail(MC_ERR_INVALID, "ragged handle is NULL");
     if (K < 0) return fail(MC_ERR_INVALID, "K < 0");
     if (K == 0 || mc_ragged_total_envs(r) == 0) return MC_OK;

@@ -356,6 +356,7 @@ void launcher_main(mc_server* s) {
             reqs = take_batch(s);
         }
         Slot& sl = s->slots[si];
+        NvtxRange nvtx("mc_server launch");
         int rc = run_batch(s, sl, reqs);
         const int rc_fin = finish_batch(s, sl, rc == MC_OK && sl.step_launch);
         if (rc == MC_OK) rc = rc_fin;
@@ -383,6 +384,7 @@ void completer_main(mc_server* s) {
         cudaError_t ce;
         while ((ce = cudaEventQuery(sl.ev)) == cudaErrorNotReady) std::this_thread::yield();
         const Clock::time_point t = Clock::now();
+        NvtxRange nvtx("mc_server complete");
         std::lock_guard<std::mutex> lk(s->mu);
         int nsteps = 0;
         for (size_t i = 0; i < sl.reqs.size(); ++i) {

@@ -506,6 +506,7 @@ void obs_to_policy(torch::Tensor obs, torch::Tensor out, int64_t layout) {
 void env_render(std::shared_ptr<Env> e) { ck(mc_env_render(e->h, cur_stream()), "render"); }
 
 void env_set_regen_mode(std::shared_ptr<Env> e, int mode) { ck(mc_env_set_regen_mode(e->h, mode), "set_regen_mode"); }
+void env_set_wait_limit(std::shared_ptr<Env> e, int polls) { ck(mc_env_set_wait_limit(e->h, polls), "set_wait_limit"); }
 
 void env_regenerate_if(std::shared_ptr<Env> e, torch::Tensor flag) {
     TORCH_CHECK(flag.is_cuda() && flag.numel() >= 1 && flag.element_size() == 1,
@@ -735,6 +736,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     m.def("obs_to_policy", &obs_to_policy);
     m.def("env_render", &env_render);
     m.def("env_set_regen_mode", &env_set_regen_mode);
+    m.def("env_set_wait_limit", &env_set_wait_limit);
     m.def("env_regenerate_if", &env_regenerate_if);
     m.def("env_rollout", &env_rollout, py::arg("env"), py::arg("actions"), py::arg("rewards_out") = py::none(),
           py::arg("dones_out") = py::none());

@@ -395,6 +395,14 @@ class MineEnv:
         _C.env_set_regen_mode(self._env, REGEN_MODES[mode])
         self.regen = mode
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Budget of the fused kernels' bounded waits for a world's bulk copy
+        into shared memory: polls > 0 polls, 0 = give up at once (every wait
+        runs out: a test of the timeout path, after which the kernel renders
+        from global memory and check_error() reports the timeout), < 0 = the
+        default."""
+        _C.env_set_wait_limit(self._env, int(polls))
+
     def regenerate_if(self, flag: torch.Tensor) -> None:
         """Regenerate every world when the one-byte device tensor `flag` is
         non-zero, with no host synchronisation (the all-reduced any-done

@@ -114,6 +114,7 @@ _PROTOS = {
     "mc_env_set_regen_mode": (I, [P, ctypes.c_int32]),
     "mc_obs_to_policy": (I, [P, P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]),
     "mc_env_get_regen_mode": (I, [P]),
+    "mc_env_set_wait_limit": (I, [P, ctypes.c_int32]),
     "mc_env_regenerate_if": (I, [P, P, P]),
     "mc_env_rollout": (I, [P, P, I, P, P, P]),
     "mc_env_rollout_prepare": (I, [P, P, I, P, P]),
