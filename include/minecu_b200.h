@@ -203,6 +203,24 @@ int mc_env_set_fused_config(mc_env* env, const mc_fused_config* cfg);
 int mc_env_get_fused_config(const mc_env* env, mc_fused_config* cfg);
 /* Reads and clears the device error word (synchronises the stream). */
 int mc_env_check_error(mc_env* env, void* stream);
+
+/* ---- debug build (no counterpart in the reference, which checks no
+ * index: src/kernels.cu:2087-2091) -------------------------------------
+ * libminecu_b200_checked.so is this library compiled with every voxel,
+ * shared-memory world, table and observation index checked against its
+ * buffer before the access (including the ray march's load one step past
+ * the staged world, which must stay within the layer of padding kept around
+ * it); a failed check skips the access and is recorded, never trapped, and
+ * the step kernels also set the env's error word (mc_env_check_error).
+ * mc_build_checks_bounds() is 1 there, 0 in libminecu_b200.so.
+ * mc_debug_bounds_report reads and clears the record of one numerics back
+ * end: out[0] violations, out[1] first site, out[2] its index, out[3] the
+ * limit it broke; MC_ERR_UNSUPPORTED in the normal build.
+ * mc_debug_bounds_selftest records one violation at site 0 with no memory
+ * access behind it, to show that a violation reaches the record. */
+int mc_build_checks_bounds(void);
+int mc_debug_bounds_report(int32_t numerics, int32_t* out, void* stream);
+int mc_debug_bounds_selftest(int32_t numerics, void* stream);
 /* Bytes of dynamic shared memory the fused kernel uses per CTA. */
 int64_t mc_env_fused_smem_bytes(const mc_env* env);
 /* The launch shape mc_env_create would choose for this configuration on a

@@ -5,6 +5,9 @@
                             mc_fast.cu is compiled with --use_fast_math (the
                             reference's numerics), mc_ieee.cu with -fmad=false
                             (IEEE numerics), mc_runtime.cu with defaults.
+  minecu/libminecu_b200_checked.so
+                            the same library with every index bounds-checked
+                            (-DMC_CHECK_BOUNDS=1): a debug build for tests.
   minecu/_C*.so             torch extension (minecu._C) binding tensors to the
                             C-ABI; linked against libminecu_b200.so.
 
@@ -26,6 +29,7 @@ OUT = os.path.join(PKG_ROOT, "minecu")
 BUILD = os.path.join(PKG_ROOT, "_build")
 INCLUDE = os.path.join(REPO, "include")
 LIB = os.path.join(OUT, "libminecu_b200.so")
+CHECKED_LIB = os.path.join(OUT, "libminecu_b200_checked.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC] + ARCH
@@ -65,21 +69,26 @@ def _run(cmd, verbose):
     subprocess.run(cmd, check=True)
 
 
-def build_lib(verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build_lib(verbose: bool = False, checked: bool = False) -> str:
+    bdir = os.path.join(BUILD, "checked") if checked else BUILD
+    lib = CHECKED_LIB if checked else LIB
+    os.makedirs(bdir, exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
     objs = []
+    extra = ["-DMC_CHECK_BOUNDS=1"] if checked else []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit + ".cu")
-        obj = os.path.join(BUILD, unit + ".o")
+        obj = os.path.join(bdir, unit + ".o")
         objs.append(obj)
         if _stale(obj, [src] + hdrs):
-            _run([nvcc] + NVCC_COMMON + flags + ["-c", src, "-o", obj], verbose)
-    if _stale(LIB, objs):
-        _run([nvcc] + ARCH + ["-shared", "-Xlinker", "-soname=libminecu_b200.so", "-o", LIB] + objs +
-             ["-lcudart_static", "-lrt", "-ldl", "-lpthread"], verbose)
-    return LIB
+            _run([nvcc] + NVCC_COMMON + flags + extra + ["-c", src, "-o", obj], verbose)
+    if _stale(lib, objs):
+        # -Bsymbolic: the library's own calls bind to its own functions, so the
+        # normal and the checked build can be loaded into one process
+        _run([nvcc] + ARCH + ["-shared", "-Xlinker", "-soname=" + os.path.basename(lib), "-Xlinker", "-Bsymbolic",
+                              "-o", lib] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"], verbose)
+    return lib
 
 
 def build_torch_ext(verbose: bool = False) -> str:
@@ -118,6 +127,7 @@ def build_torch_ext(verbose: bool = False) -> str:
 def build(verbose: bool = False) -> None:
     build_lib(verbose)
     build_torch_ext(verbose)
+    build_lib(verbose, checked=True)
 
 
 if __name__ == "__main__":

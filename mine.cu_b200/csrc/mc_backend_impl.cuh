@@ -98,6 +98,42 @@ struct N {
 #endif
 
 // ---------------------------------------------------------------------------
+// Bounds checks of the debug build (MC_CHECK_BOUNDS=1)
+// ---------------------------------------------------------------------------
+// In the debug build every voxel, shared-memory world, table and observation
+// index is checked against its buffer before the access.  A failed check
+// skips the access (a voxel read returns air) and records the first
+// violation (site, index, limit) and a count in g_bounds, which
+// bounds_report() reads and clears; the step kernels also set
+// MC_KERR_BOUNDS in their env's error word.  Nothing traps.  The normal
+// build compiles every check to nothing.
+#ifndef MC_CHECK_BOUNDS
+#define MC_CHECK_BOUNDS 0
+#endif
+#if MC_CHECK_BOUNDS
+__device__ int32_t g_bounds[4];  // violations, first site (MC_SITE_*), first index, its limit
+__device__ __noinline__ void bounds_fail(long long i, long long n, int site) {
+    if (atomicAdd(&g_bounds[0], 1) == 0) {
+        g_bounds[1] = site;
+        g_bounds[2] = (int32_t)i;
+        g_bounds[3] = (int32_t)n;
+    }
+}
+__device__ __forceinline__ bool in_bounds(long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    bounds_fail(i, n, site);
+    return false;
+}
+// A step kernel's exit: a violation anywhere is also reported in the env's error word.
+__device__ __forceinline__ void bounds_to_flags(int32_t* flags) {
+    if (*(volatile int32_t*)&g_bounds[0]) atomicCAS(&flags[MC_FLAG_ERROR], MC_KERR_NONE, MC_KERR_BOUNDS);
+}
+#else
+__device__ __forceinline__ constexpr bool in_bounds(long long, long long, int) { return true; }
+__device__ __forceinline__ void bounds_to_flags(int32_t*) {}
+#endif
+
+// ---------------------------------------------------------------------------
 // Agent step
 // ---------------------------------------------------------------------------
 struct Dec {
@@ -295,7 +331,7 @@ __device__ __forceinline__ int interact_seq(int8_t* w, const Agent& a, bool brk,
     int prev = -1;
     for (int k = 0; k < 32; ++k) {
         Sample s = interact_sample(k, eye_x, eye_y, eye_z, dx, dy, dz, p.wx, p.wy, p.wz);
-        if (s.inb) {
+        if (s.inb && in_bounds(s.idx, (long long)p.wx * p.wy * p.wz, MC_SITE_INTERACT)) {
             int8_t blk = w[s.idx];
             if (blk >= 0) {
                 if (brk) {
@@ -328,7 +364,7 @@ __device__ __forceinline__ int interact_warp(int8_t* w, const Agent& a, bool brk
     float dx, dy, dz;
     interact_dir(a, dx, dy, dz);
     Sample s = interact_sample(lane, a.x, N::add(a.y, 1.6f), a.z, dx, dy, dz, p.wx, p.wy, p.wz);
-    int8_t blk = s.inb ? w[s.idx] : AIR;
+    int8_t blk = (s.inb && in_bounds(s.idx, (long long)p.wx * p.wy * p.wz, MC_SITE_INTERACT)) ? w[s.idx] : AIR;
     unsigned solid = __ballot_sync(0xffffffffu, s.inb && blk >= 0);
     unsigned inbm = __ballot_sync(0xffffffffu, s.inb);
     if (solid == 0u) return -1;
@@ -506,18 +542,28 @@ __device__ __forceinline__ float v_prebasis(int py, int height, float scale_v) {
     return N::mul(N::one_sub_div(N::mul(2.0f, N::add((float)py, 0.5f)), (float)height), scale_v);
 }
 
-// Voxel sources for the ray march.
+// Voxel sources for the ray march.  at(idx, n): the voxel at idx of a world
+// of n voxels (bounds-checked in the debug build).
 struct VoxGlobal {
     const int8_t* w;
     __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+    __device__ __forceinline__ int8_t at(int idx, int n) const {
+        return in_bounds(idx, n, MC_SITE_MARCH_GLOBAL) ? w[idx] : (int8_t)-1;
+    }
 };
 struct VoxLdg {  // read-only world (plain render kernels): the reference's __ldg path
     const int8_t* w;
     __device__ __forceinline__ int8_t operator()(int idx) const { return __ldg(w + idx); }
+    __device__ __forceinline__ int8_t at(int idx, int n) const {
+        return in_bounds(idx, n, MC_SITE_MARCH_GLOBAL) ? __ldg(w + idx) : (int8_t)-1;
+    }
 };
 struct VoxShared {
     const int8_t* w;
     __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+    __device__ __forceinline__ int8_t at(int idx, int n) const {
+        return in_bounds(idx, n, MC_SITE_MARCH_SHARED) ? w[idx] : (int8_t)-1;
+    }
 };
 // Either source behind one generic pointer (one call site for both), with a
 // per-env flag telling whether it points into shared memory.
@@ -525,6 +571,9 @@ struct VoxEither {
     const int8_t* w;
     bool smem;
     __device__ __forceinline__ int8_t operator()(int idx) const { return w[idx]; }
+    __device__ __forceinline__ int8_t at(int idx, int n) const {
+        return in_bounds(idx, n, smem ? MC_SITE_MARCH_SHARED : MC_SITE_MARCH_GLOBAL) ? w[idx] : (int8_t)-1;
+    }
 };
 
 struct Hit {
@@ -555,10 +604,86 @@ struct Hit {
 // after the staged world, which the shared-memory layouts keep allocated
 // (the value read there is not used).
 // Returns the block hit (>= 0), or -1 when the ray left the box.
+// The debug build's marches (below) also check every load address against
+// `chk` (the staged world and one layer on either side: the march's own
+// claim) and against the CTA's dynamic shared memory.
+struct SmemRange {
+    uint32_t lo, span;  // shared-memory addresses [lo, lo + span)
+};
+__device__ __forceinline__ SmemRange staged_range(uint32_t base, int wxz, int nvox) {
+    return SmemRange{base - (uint32_t)wxz, (uint32_t)(nvox + 2 * wxz)};
+}
+#if MC_CHECK_BOUNDS
+extern __shared__ __align__(16) uint8_t mc_dyn_smem[];
+__device__ __forceinline__ SmemRange dyn_smem_range() {
+    uint32_t n;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(n));
+    return SmemRange{(uint32_t)__cvta_generic_to_shared(mc_dyn_smem), n};
+}
+// A failed check of a PTX march's load address a: which range it left.
+__device__ __noinline__ void march_bounds_fail(uint32_t a, SmemRange chk, int site) {
+    const SmemRange d = dyn_smem_range();
+    if (a - d.lo >= d.span) bounds_fail((long long)a - d.lo, d.span, MC_SITE_MARCH_SMEM);
+    else bounds_fail((long long)a - chk.lo, chk.span, site);
+}
+#endif
+
 __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, int px, int py, int pz, float& tmx,
-                                                   float& tmy, float& tmz, float tdx, float tdy, float tdz) {
+                                                   float& tmy, float& tmz, float tdx, float tdy, float tdz,
+                                                   SmemRange chk = SmemRange{0u, 0u}) {
     constexpr int kGuard = (32 << 12) | (32 << 6) | 32;
     int b;
+#if MC_CHECK_BOUNDS
+    const SmemRange dyn = dyn_smem_range();
+    uint32_t bad = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq, pb1, pb2;\n\t"
+        ".reg .b32 ra, rc;\n\t"
+        ".reg .s32 rv;\n\t"
+        "MC_CMARCH_LOOP:\n\t"
+        "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pby|pzy, %2, %3, pna;\n\t"
+        "or.pred pz, pzx, pzy;\n\t"
+        "@pbx add.s32 %4, %4, %6;\n\t"
+        "@pby add.s32 %4, %4, %7;\n\t"
+        "@pz add.s32 %4, %4, %8;\n\t"
+        "shr.s32 ra, %4, 18;\n\t"
+        "add.s32 ra, ra, %10;\n\t"
+        "sub.u32 rc, ra, %15;\n\t"
+        "setp.ge.u32 pb1, rc, %16;\n\t"
+        "sub.u32 rc, ra, %17;\n\t"
+        "setp.ge.u32 pb2, rc, %18;\n\t"
+        "or.pred pb1, pb1, pb2;\n\t"
+        "@pb1 mov.u32 %5, ra;\n\t"
+        "@pb1 mov.s32 %0, -2;\n\t"
+        "@pb1 bra MC_CMARCH_END;\n\t"
+        "ld.shared.s8 rv, [ra];\n\t"
+        "lop3.b32 ra, %4, rv, %9, 0xA2;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "@pq bra MC_CMARCH_DONE;\n\t"
+        "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %11;\n\t"
+        "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %12;\n\t"
+        "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %13;\n\t"
+        "bra MC_CMARCH_LOOP;\n\t"
+        "MC_CMARCH_DONE:\n\t"
+        "and.b32 ra, %4, %14;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "selp.b32 %0, -1, rv, pq;\n\t"
+        "MC_CMARCH_END:\n\t"
+        "}"
+        : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(packed), "+r"(bad)
+        : "r"(px), "r"(py), "r"(pz), "n"(kGuard | (int)0x80000000u), "r"(world), "f"(tdx), "f"(tdy), "f"(tdz),
+          "n"(kGuard), "r"(chk.lo), "r"(chk.span), "r"(dyn.lo), "r"(dyn.span)
+        : "memory");
+    if (b == -2) {  // a load address outside its range: the load was skipped, the ray ends as sky
+        march_bounds_fail(bad, chk, MC_SITE_MARCH_PACKED);
+        b = -1;
+    }
+    return b;
+#else
+    (void)chk;
     asm volatile(
         "{\n\t"
         ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
@@ -594,6 +719,7 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
           "n"(kGuard)
         : "memory");
     return b;
+#endif
 }
 
 // Start values of march_packed_shared for an env whose eye is in voxel
@@ -628,8 +754,62 @@ __device__ __forceinline__ int split_counts(int cx, int cy, int cz, int max_step
 // distances left at a hit as in march_packed_shared.  Returns the block hit
 // (>= 0), or -1 when the ray left the box or ran out of steps.
 __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int dax, int day, int daz, float& tmx,
-                                                  float& tmy, float& tmz, float tdx, float tdy, float tdz) {
+                                                  float& tmy, float& tmz, float tdx, float tdy, float tdz,
+                                                  SmemRange chk = SmemRange{0u, 0u}) {
     int b;
+#if MC_CHECK_BOUNDS
+    const SmemRange dyn = dyn_smem_range();
+    uint32_t bad = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq, pb1, pb2;\n\t"
+        ".reg .b32 ra, rc;\n\t"
+        ".reg .s32 rv;\n\t"
+        "MC_CSPLIT_LOOP:\n\t"
+        "setp.lt" MC_PTX_FTZ ".f32 pa|pna, %1, %2;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pbx|pzx, %1, %3, pa;\n\t"
+        "setp.lt.and" MC_PTX_FTZ ".f32 pby|pzy, %2, %3, pna;\n\t"
+        "or.pred pz, pzx, pzy;\n\t"
+        "@pbx add.s32 %4, %4, %7;\n\t"
+        "@pby add.s32 %4, %4, %8;\n\t"
+        "@pz add.s32 %4, %4, %9;\n\t"
+        "@pbx add.s32 %5, %5, %10;\n\t"
+        "@pby add.s32 %5, %5, %11;\n\t"
+        "@pz add.s32 %5, %5, %12;\n\t"
+        "sub.u32 rc, %4, %18;\n\t"
+        "setp.ge.u32 pb1, rc, %19;\n\t"
+        "sub.u32 rc, %4, %20;\n\t"
+        "setp.ge.u32 pb2, rc, %21;\n\t"
+        "or.pred pb1, pb1, pb2;\n\t"
+        "@pb1 mov.u32 %6, %4;\n\t"
+        "@pb1 mov.s32 %0, -2;\n\t"
+        "@pb1 bra MC_CSPLIT_END;\n\t"
+        "ld.shared.s8 rv, [%4];\n\t"
+        "lop3.b32 ra, %5, rv, %13, 0xA2;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "@pq bra MC_CSPLIT_DONE;\n\t"
+        "@pbx add.rn" MC_PTX_FTZ ".f32 %1, %1, %14;\n\t"
+        "@pby add.rn" MC_PTX_FTZ ".f32 %2, %2, %15;\n\t"
+        "@pz add.rn" MC_PTX_FTZ ".f32 %3, %3, %16;\n\t"
+        "bra MC_CSPLIT_LOOP;\n\t"
+        "MC_CSPLIT_DONE:\n\t"
+        "and.b32 ra, %5, %17;\n\t"
+        "setp.ne.b32 pq, ra, 0;\n\t"
+        "selp.b32 %0, -1, rv, pq;\n\t"
+        "MC_CSPLIT_END:\n\t"
+        "}"
+        : "=&r"(b), "+f"(tmx), "+f"(tmy), "+f"(tmz), "+r"(addr), "+r"(cnt), "+r"(bad)
+        : "r"(dax), "r"(day), "r"(daz), "n"((1 << 7) | (1 << 21)), "n"((1 << 14) | (1 << 21)), "n"(1 | (1 << 21)),
+          "n"(kSplitGuard | (int)0x80000000u), "f"(tdx), "f"(tdy), "f"(tdz), "n"(kSplitGuard), "r"(chk.lo),
+          "r"(chk.span), "r"(dyn.lo), "r"(dyn.span)
+        : "memory");
+    if (b == -2) {
+        march_bounds_fail(bad, chk, MC_SITE_MARCH_SPLIT);
+        b = -1;
+    }
+    return b;
+#else
+    (void)chk;
     asm volatile(
         "{\n\t"
         ".reg .pred pa, pna, pbx, pzx, pby, pzy, pz, pq;\n\t"
@@ -665,6 +845,7 @@ __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int da
           "n"(kSplitGuard | (int)0x80000000u), "f"(tdx), "f"(tdy), "f"(tdz), "n"(kSplitGuard)
         : "memory");
     return b;
+#endif
 }
 
 // March from the eye's voxel (index idx, in-box steps left cx, cy, cz) through
@@ -673,13 +854,14 @@ __device__ __forceinline__ int march_split_shared(uint32_t addr, int cnt, int da
 __device__ __forceinline__ int march_staged(uint32_t base, int idx, int cx, int cy, int cz, int dix, int diy, int diz,
                                            int wx, int wy, int wz, int max_steps, float& tmx, float& tmy, float& tmz,
                                            float tdx, float tdy, float tdz) {
+    const SmemRange chk = staged_range(base, wx * wz, wx * wy * wz);
     if (max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 && wx * wy * wz < 8192) {
         const int packed = (idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz);
         return march_packed_shared(base, packed, (dix << 18) + (1 << 12), (diy << 18) + (1 << 6), (diz << 18) + 1,
-                                   tmx, tmy, tmz, tdx, tdy, tdz);
+                                   tmx, tmy, tmz, tdx, tdy, tdz, chk);
     }
     return march_split_shared(base + idx, split_counts(cx, cy, cz, max_steps, wx, wy, wz), dix, diy, diz, tmx, tmy,
-                              tmz, tdx, tdy, tdz);
+                              tmz, tdx, tdy, tdz, chk);
 }
 
 // Whether a march can run on the staged copy: V is a shared-memory source
@@ -791,6 +973,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
     float t = 0.0f;
     int face = -1;
     const int wxz = wx * wz;
+    const int nvox = wxz * wy;  // for the debug build's checks
     // linear voxel index kept in step with (vx, vy, vz)
     int idx = vy * wxz + vx * wz + vz;
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
@@ -806,7 +989,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             // reference had already ended the ray as sky (its `t >= vd`
             // break); a ray that leaves the box or runs out of steps is sky
             // in both.
-            int b = skip_first ? (int)AIR : (int)vox(idx);
+            int b = skip_first ? (int)AIR : (int)vox.at(idx, nvox);
             // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
             const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
                       cz = (sz > 0) ? wz - 1 - vz : vz;
@@ -815,16 +998,18 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 if (TAB && start) {
                     // the env's start values for this ray's signs
                     const int4 e = start[(ray_x >= 0.0f ? 1 : 0) | (ray_y >= 0.0f ? 2 : 0) | (ray_z >= 0.0f ? 4 : 0)];
-                    b = march_packed_shared(base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz);
+                    b = march_packed_shared(base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz,
+                                            staged_range(base, wxz, nvox));
                 } else if (vd_safe && max_steps > wx + wy + wz && wx <= 31 && wy <= 31 && wz <= 31 &&
                            wx * wy * wz < 8192) {
                     // index and in-box counts in one register (march_packed_shared)
                     const int packed = (idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz);
                     b = march_packed_shared(base, packed, (dix << 18) + (1 << 12), (diy << 18) + (1 << 6),
-                                            (diz << 18) + 1, tmx, tmy, tmz, tdx, tdy, tdz);
+                                            (diz << 18) + 1, tmx, tmy, tmz, tdx, tdy, tdz,
+                                            staged_range(base, wxz, nvox));
                 } else {
                     b = march_split_shared(base + idx, split_counts(cx, cy, cz, max_steps, wx, wy, wz), dix, diy,
-                                           diz, tmx, tmy, tmz, tdx, tdy, tdz);
+                                           diz, tmx, tmy, tmz, tdx, tdy, tdz, staged_range(base, wxz, nvox));
                 }
                 if (b >= 0) {
                     // the axis of the last step, chosen again from the same distances
@@ -848,7 +1033,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         // turns; one test per iteration ends the loop (hit, left the box, or
         // max_steps).  The eye's voxel is inside the box.
         int8_t b = AIR;
-        if (!skip_first && max_steps > 0) b = vox(idx);
+        if (!skip_first && max_steps > 0) b = vox.at(idx, nvox);
         bool lbx = false, lby = false, adv = false;
         // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
         int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
@@ -879,7 +1064,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 lby = by;
                 adv = true;
                 if (packed & kGuard) break;
-                b = vox(packed >> 18);
+                b = vox.at(packed >> 18, nvox);
             }
         } else {
             while (b < 0 && max_steps > 0) {
@@ -899,7 +1084,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
                 lby = by;
                 adv = true;
                 if ((cx | cy | cz) < 0 || ++step >= max_steps) break;
-                b = vox(idx);
+                b = vox.at(idx, nvox);
             }
         }
         if (adv) face = lbx ? 0 : (lby ? 1 : 2);
@@ -913,7 +1098,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
         // count in its single exit test (worlds whose far corners lie beyond
         // view_distance)
         int8_t b = AIR;
-        if (!skip_first) b = vox(idx);
+        if (!skip_first) b = vox.at(idx, nvox);
         bool lbx = false, lby = false, adv = false;
         // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
         int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
@@ -935,7 +1120,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             lby = by;
             adv = true;
             if ((cx | cy | cz) < 0 || ++step >= max_steps || t >= vd) break;
-            b = vox(idx);
+            b = vox.at(idx, nvox);
         }
         if (adv) face = lbx ? 0 : (lby ? 1 : 2);
         h.blk = (b >= 0) ? (int)b : AIR;
@@ -960,7 +1145,7 @@ __device__ __forceinline__ Hit shade_ray(const Cam& c, const Dda0& d0, float u, 
             break;
         }
         if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
-            int8_t b = vox(idx);
+            int8_t b = vox.at(idx, nvox);
             if (b >= 0) {
                 h.blk = b;
                 break;
@@ -1018,7 +1203,7 @@ __device__ __forceinline__ int sky_fused_mask(int kind) {
 template <int KIND>
 __device__ __forceinline__ void shade_rgb(const Hit& h, float vd, float rcp_vd, const float (*rgb)[3], const float* sky,
                                           float out[3]) {
-    if (h.blk >= 0) {
+    if (h.blk >= 0 && in_bounds(h.blk, 13, MC_SITE_TABLE)) {
         float r = rgb[h.blk][0], g = rgb[h.blk][1], b_col = rgb[h.blk][2];
         float shade = 1.0f;
         if (h.face == 0) shade = 0.8f;
@@ -1069,6 +1254,7 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
     ray_y = N::mul(ray_y, ray_len);
     ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
+    const int nvox = wxz * wy;  // for the debug build's checks
     int vx = d0.vx, vy = d0.vy, vz = d0.vz;
     int sx = (ray_x >= 0) ? 1 : -1;
     int sy = (ray_y >= 0) ? 1 : -1;
@@ -1090,14 +1276,15 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
     const int dix = sx * wz, diy = sy * wxz, diz = sz;
     if (sky_exit && max_steps > 0 && staged_source(vox, wx, wy, wz)) {
         // the PTX marches over the staged world (as in shade_ray, no view distance)
-        int b = skip_first ? (int)AIR : (int)vox(idx);
+        int b = skip_first ? (int)AIR : (int)vox.at(idx, nvox);
         if (b < 0) {
             // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
             const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
                       cz = (sz > 0) ? wz - 1 - vz : vz;
             if (TAB && start) {
                 const int4 e = start[(ray_x >= 0.0f ? 1 : 0) | (ray_y >= 0.0f ? 2 : 0) | (ray_z >= 0.0f ? 4 : 0)];
-                b = march_packed_shared(staged_base(vox), e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz);
+                b = march_packed_shared(staged_base(vox), e.x, e.y, e.z, e.w, tmx, tmy, tmz, tdx, tdy, tdz,
+                                        staged_range(staged_base(vox), wxz, nvox));
             } else {
                 b = march_staged(staged_base(vox), idx, cx, cy, cz, dix, diy, diz, wx, wy, wz, max_steps, tmx, tmy,
                                  tmz, tdx, tdy, tdz);
@@ -1115,7 +1302,7 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
         // branch-free axis choice as in shade_ray; one exit test per iteration
         int8_t b = AIR;
         int step = 0;
-        if (!skip_first && max_steps > 0) b = vox(idx);
+        if (!skip_first && max_steps > 0) b = vox.at(idx, nvox);
         while (b < 0 && max_steps > 0) {
             const bool bx = tmx < tmy && tmx < tmz;
             const bool by = !bx && tmy < tmz;
@@ -1131,7 +1318,7 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
             face = bx ? 0 : (by ? 1 : 2);
             const bool out = (unsigned)vx >= (unsigned)wx || (unsigned)vy >= (unsigned)wy || (unsigned)vz >= (unsigned)wz;
             if (out || ++step >= max_steps) break;
-            b = vox(idx);
+            b = vox.at(idx, nvox);
         }
         h.blk = (b >= 0) ? (int)b : AIR;
         h.face = face;
@@ -1141,7 +1328,7 @@ __device__ __forceinline__ Hit flat_ray(const Cam& c, const Dda0& d0, float u, f
         // skip_first: the eye's voxel is known to be air or outside the world
         if ((step > 0 || !skip_first) &&
             (unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
-            int8_t b = vox(idx);
+            int8_t b = vox.at(idx, nvox);
             if (b >= 0) {
                 h.blk = b;
                 break;
@@ -1171,6 +1358,7 @@ __device__ __forceinline__ Hit fp16_ray(const Cam& c, const Dda0& d0, float u, f
     ray_y = N::mul(ray_y, ray_len);
     ray_z = N::mul(ray_z, ray_len);
     int wxz = wx * wz;
+    const int nvox = wxz * wy;  // for the debug build's checks
     int vx = d0.vx, vy = d0.vy, vz = d0.vz;
     int sx = (ray_x >= 0) ? 1 : -1;
     int sy = (ray_y >= 0) ? 1 : -1;
@@ -1192,7 +1380,7 @@ __device__ __forceinline__ Hit fp16_ray(const Cam& c, const Dda0& d0, float u, f
     int face = -1;
     for (int step = 0; step < max_steps; ++step) {
         if ((unsigned)vx < (unsigned)wx && (unsigned)vy < (unsigned)wy && (unsigned)vz < (unsigned)wz) {
-            int8_t b = vox(vy * wxz + vx * wz + vz);
+            int8_t b = vox.at(vy * wxz + vx * wz + vz, nvox);
             if (b >= 0) {
                 h.blk = b;
                 break;
@@ -1391,7 +1579,7 @@ __global__ void __launch_bounds__(128) k_render_flat(mc_kp p) {
     else h = flat_ray<true>(c, d0, u, v, vox, p.wx, p.wy, p.wz, p.max_steps);
     long long o = (b * hw + pix);
     uint8_t* out = (uint8_t*)p.obs + o * 3;
-    const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
+    const uint8_t* col = (h.blk >= 0 && in_bounds(h.blk, 13, MC_SITE_TABLE)) ? c_rgb8[h.blk] : c_sky8;
     out[0] = col[0]; out[1] = col[1]; out[2] = col[2];
     if (p.dbg_pixel) p.dbg_pixel[o] = dbg_code(h);
 }
@@ -1417,9 +1605,12 @@ __global__ void __launch_bounds__(128) k_render_coalesced(const int8_t* vox, con
             // idx = y*ws*ws + x*ws + z  ->  [y][x][z][b]
             return __ldg(v + (long long)idx * B + b);
         }
+        __device__ __forceinline__ int8_t at(int idx, int n) const {
+            return in_bounds(idx, n, MC_SITE_MARCH_GLOBAL) ? (*this)(idx) : (int8_t)-1;
+        }
     } acc{vox, B, b, ws};
     Hit h = flat_ray<false>(c, dda0(c), u, v, acc, ws, ws, ws, max_steps);
-    const uint8_t* col = (h.blk >= 0) ? c_rgb8[h.blk] : c_sky8;
+    const uint8_t* col = (h.blk >= 0 && in_bounds(h.blk, 13, MC_SITE_TABLE)) ? c_rgb8[h.blk] : c_sky8;
     uint8_t* o = out + ((long long)b * H * W + pix) * 3;
     o[0] = col[0]; o[1] = col[1]; o[2] = col[2];
 }
@@ -1764,7 +1955,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         int eye_idx = ey * wxz + ex * p.wz + ez;
         int8_t eye_blk = AIR;
         __syncwarp();
-        if (eye_inb) eye_blk = gw[eye_idx];
+        if (eye_inb && in_bounds(eye_idx, wxyz, MC_SITE_EYE)) eye_blk = gw[eye_idx];
         bool inside = false;
         bool buried;
         int fill_blk = eye_blk;
@@ -1843,6 +2034,16 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         const int8_t* wsrc = gw;
         int ytop = p.wy - 1;  // highest layer with a solid voxel (all layers unless measured)
         if (STAGE) {
+#if MC_CHECK_BOUNDS
+            {
+                const SmemRange dyn = dyn_smem_range();
+                const long long off = (long long)smem_u32(sworld) - dyn.lo;
+                if (!in_bounds(off, dyn.span, MC_SITE_STAGE) || !in_bounds(off + wxyz - 1, dyn.span, MC_SITE_STAGE)) {
+                    no_stage = true;  // no copy issued: render from global memory
+                    break;
+                }
+            }
+#endif
             if (lane == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_a), "r"(wxyz)
@@ -1862,7 +2063,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
             }
             phase ^= 1u;
             // the interaction may have written after the copy read the byte
-            if (lane == 0 && mod_idx >= 0) sworld[mod_idx] = mod_val;
+            if (lane == 0 && mod_idx >= 0 && in_bounds(mod_idx, wxyz, MC_SITE_PATCH)) sworld[mod_idx] = mod_val;
             __syncwarp();
             wsrc = sworld;
             ytop = staged_top_layer(sworld, p.wx, p.wy, p.wz, lane);
@@ -1889,10 +2090,10 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         const int bpp = 3 * (F32 ? 4 : 1);  // bytes per pixel
         for (int row0 = 0; row0 < H; row0 += TH) {
             const int py = row0 + ly;
-            const float v = (py < H) ? s_v[py] : 0.0f;
+            const float v = (py < H && in_bounds(py, H, MC_SITE_TABLE)) ? s_v[py] : 0.0f;
             for (int tx0 = 0; tx0 < W; tx0 += TW) {
                 const int px = tx0 + lx;
-                if (px < W && py < H) {
+                if (px < W && py < H && in_bounds(px, W, MC_SITE_TABLE)) {
                     Hit h;
                     const float u = s_u[px];
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
@@ -1909,6 +2110,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                         else h = flat_ray<TRIG>(c, d0, u, v, VoxGlobal{wsrc}, p.wx, p.wy, p.wz, p.max_steps, skip_first, sky_exit);
                     }
                     const int so = ly * W + px;  // pixel within the staged band
+                    if (!in_bounds((long long)(so + 1) * bpp - 1, L.stage_bytes, MC_SITE_BAND)) continue;
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         float rgb[3];
                         shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
@@ -1923,17 +2125,23 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                             sb[2] = (uint8_t)to_u8(rgb[2]);
                         }
                     } else {
-                        const uint8_t* col = (h.blk >= 0) ? s_rgb8[h.blk] : s_sky8;
+                        const uint8_t* col = (h.blk >= 0 && in_bounds(h.blk, 13, MC_SITE_TABLE)) ? s_rgb8[h.blk] : s_sky8;
                         uint8_t* sb = stage + so * 3;
                         sb[0] = col[0]; sb[1] = col[1]; sb[2] = col[2];
                     }
-                    if (p.dbg_pixel) p.dbg_pixel[e * HW + py * W + px] = dbg_code(h);
+                    if (p.dbg_pixel && in_bounds(py * W + px, HW, MC_SITE_DEBUG))
+                        p.dbg_pixel[e * HW + py * W + px] = dbg_code(h);
                 }
             }
             __syncwarp();
             // copy the band (rows row0 .. row0+TH-1) out
             const int nbytes = min(TH, H - row0) * W * bpp;
             uint8_t* dst = oenv + (long long)row0 * W * bpp;
+            if (!in_bounds((long long)row0 * W * bpp + nbytes - 1, obs_env_bytes, MC_SITE_COPY_OUT) ||
+                !in_bounds(nbytes - 1, L.stage_bytes, MC_SITE_BAND)) {
+                __syncwarp();
+                continue;
+            }
             if (vec_ok && (nbytes & 15) == 0 && (((long long)row0 * W * bpp) & 15) == 0) {
                 const uint4* s4 = reinterpret_cast<const uint4*>(stage);
                 uint4* d4 = reinterpret_cast<uint4*>(dst);
@@ -1961,6 +2169,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     }
     // No CTA barrier here: warps leave as soon as their last env is done.
     if (lane == 0) {
+        bounds_to_flags(p.flags);
         if (any_done) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
         if (p.sched_dynamic) {
             // every claim of this warp has returned (the last one >= B); the
@@ -2065,7 +2274,7 @@ __device__ __forceinline__ EnvRender agent_step(const mc_kp& p, const ActionSrc&
     bool eye_inb = (unsigned)ex < (unsigned)p.wx && (unsigned)ey < (unsigned)p.wy && (unsigned)ez < (unsigned)p.wz;
     int8_t eye_blk = AIR;
     __syncwarp();
-    if (eye_inb) eye_blk = gw[ey * wxz + ex * p.wz + ez];
+    if (eye_inb && in_bounds(ey * wxz + ex * p.wz + ez, wxyz, MC_SITE_EYE)) eye_blk = gw[ey * wxz + ex * p.wz + ez];
     bool inside = false, buried, skip_first;
     int fill_blk = eye_blk;
     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
@@ -2196,14 +2405,15 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
     for (int b = band_ctr ? claim() : 0; b < nbands; b = band_ctr ? claim() : b + 1) {
         const int row0 = b * TH;
         const int py = row0 + ly;
-        const float v = (py < H) ? cx.s_v[py] : 0.0f;
+        const float v = (py < H && in_bounds(py, H, MC_SITE_TABLE)) ? cx.s_v[py] : 0.0f;
         for (int tx0 = 0; tx0 < W; tx0 += TW) {
             const int px = tx0 + lx;
-            if (px < W && py < H) {
+            if (px < W && py < H && in_bounds(px, W, MC_SITE_TABLE)) {
                 const float u = cx.s_u[px];
                 Hit h = march_pixel<FAM, V, VDLIM>(rp, r.c, d0, u, v, vox, inside, skip_first, sky_exit, vd_safe,
                                                    r.ytop);
                 const int so = ly * W + px;  // pixel within the staged band
+                if (!in_bounds((long long)(so + 1) * bpp - 1, (long long)TH * W * bpp, MC_SITE_BAND)) continue;
                 if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                     float rgb[3];
                     shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
@@ -2220,19 +2430,24 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
                         sb[2] = (uint8_t)to_u8(rgb[2]);
                     }
                 } else {
-                    const uint8_t* col = (h.blk >= 0) ? cx.s_rgb8[h.blk] : cx.s_sky8;
+                    const uint8_t* col = (h.blk >= 0 && in_bounds(h.blk, 13, MC_SITE_TABLE)) ? cx.s_rgb8[h.blk] : cx.s_sky8;
                     uint8_t* sb = cx.stage + so * 3;
                     sb[0] = col[0];
                     sb[1] = col[1];
                     sb[2] = col[2];
                 }
-                if (dbg_pixel) dbg_pixel[e * W * H + py * W + px] = dbg_code(h);
+                if (dbg_pixel && in_bounds(py * W + px, W * H, MC_SITE_DEBUG))
+                    dbg_pixel[e * W * H + py * W + px] = dbg_code(h);
             }
         }
         __syncwarp();
         // copy the band (rows row0 .. row0+TH-1) out
         const int nbytes = min(TH, H - row0) * W * bpp;
         uint8_t* dst = oenv + (long long)row0 * W * bpp;
+        if (!in_bounds((long long)row0 * W * bpp + nbytes - 1, obs_env_bytes, MC_SITE_COPY_OUT)) {
+            __syncwarp();
+            continue;
+        }
         if (vec_ok && (nbytes & 15) == 0 && (((long long)row0 * W * bpp) & 15) == 0) {
             const uint4* s4 = reinterpret_cast<const uint4*>(cx.stage);
             uint4* d4 = reinterpret_cast<uint4*>(dst);
@@ -2392,11 +2607,20 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                 }
             }
             staged = ((rk.stage_mask >> g) & 1) && !(r.bits & MC_ER_BURIED) && !warp_no_stage;
+#if MC_CHECK_BOUNDS
+            if (staged) {
+                const SmemRange dyn = dyn_smem_range();
+                const long long off = (long long)smem_u32(world) - dyn.lo;
+                if (!in_bounds(off, dyn.span, MC_SITE_STAGE) || !in_bounds(off + wxyz - 1, dyn.span, MC_SITE_STAGE))
+                    staged = false;  // no copy issued: render from global memory
+            }
+#endif
             if (staged) {
                 const uint32_t ph = phase;
                 if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane, p.wait_polls)) {
                     // the interaction may have written after the copy read the byte
-                    if (lane == 0 && r.mod_idx >= 0) world[r.mod_idx] = (int8_t)r.mod_val;
+                    if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
+                        world[r.mod_idx] = (int8_t)r.mod_val;
                     __syncwarp();
                     r.ytop = staged_top_layer(world, p.wx, p.wy, p.wz, lane);
                 } else {
@@ -2432,6 +2656,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     // this warp's part of shared memory can be released
     if (warp_no_stage) mbar_wait(cx.mbar_a, pending_phase);
     if (lane == 0) {
+        for (int g = 0; g < G; ++g) bounds_to_flags(rk.groups[g].flags);
         for (int g = 0; g < G; ++g)
             if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);
     }
@@ -2565,6 +2790,46 @@ static int step_fused(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cuda
         case MC_FAM_PREBASIS: return launch_fused_f<MC_FAM_PREBASIS, false>(p, cfg, num_sms, s);
         default: return (int)cudaErrorInvalidValue;
     }
+}
+
+#if MC_CHECK_BOUNDS
+// One failed check with no memory access behind it: shows that a violation
+// reaches the record (the checks themselves cannot be made to fail on
+// purpose without an out-of-range access to skip).
+__global__ void k_bounds_selftest() {
+    if (threadIdx.x == 0) (void)in_bounds(-1, 1, 0);
+}
+#endif
+static int bounds_selftest(cudaStream_t s) {
+#if MC_CHECK_BOUNDS
+    k_bounds_selftest<<<1, 32, 0, s>>>();
+    return (int)cudaGetLastError();
+#else
+    (void)s;
+    return -1;
+#endif
+}
+
+// The debug build's bounds-check record: out = {violations, first site,
+// first index, its limit}, then cleared.  -1 (and out untouched) in the
+// normal build, which checks nothing.
+static int bounds_report(int32_t out[4], cudaStream_t s) {
+#if MC_CHECK_BOUNDS
+    int32_t h[4];
+    cudaError_t e = cudaMemcpyFromSymbolAsync(h, g_bounds, sizeof(h), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return (int)e;
+    const int32_t zero[4] = {0, 0, 0, 0};
+    e = cudaMemcpyToSymbolAsync(g_bounds, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return (int)e;
+    for (int i = 0; i < 4; ++i) out[i] = h[i];
+    return 0;
+#else
+    (void)out;
+    (void)s;
+    return -1;
+#endif
 }
 
 static int basis_launch(const mc_kp* p, cudaStream_t s) {

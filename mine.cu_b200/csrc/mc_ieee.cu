@@ -20,6 +20,8 @@ static const mc_backend g_backend = {
     coalesced_launch,
     fused_smem,
     step_team,
+    bounds_report,
+    bounds_selftest,
 };
 }  // namespace mc_ieee
 

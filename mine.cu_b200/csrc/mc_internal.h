@@ -24,7 +24,25 @@ enum {
 };
 
 // Error codes a kernel can record in flags[MC_FLAG_ERROR] (never a trap).
-enum { MC_KERR_NONE = 0, MC_KERR_TMA_TIMEOUT = 1 };
+enum { MC_KERR_NONE = 0, MC_KERR_TMA_TIMEOUT = 1, MC_KERR_BOUNDS = 2 };
+
+// Places the debug build checks an index (the first violation's site is
+// reported by mc_debug_bounds_report).
+enum {
+    MC_SITE_INTERACT = 1,      // interaction samples: world voxel read/write
+    MC_SITE_EYE = 2,           // the eye's voxel
+    MC_SITE_MARCH_GLOBAL = 3,  // march over a world in global memory
+    MC_SITE_MARCH_SHARED = 4,  // march over a staged world (C++ loops)
+    MC_SITE_MARCH_PACKED = 5,  // PTX packed march: load address vs the staged world +- one layer
+    MC_SITE_MARCH_SPLIT = 6,   // PTX split march: the same
+    MC_SITE_MARCH_SMEM = 7,    // PTX marches: load address vs the CTA's dynamic shared memory
+    MC_SITE_BAND = 8,          // a pixel's bytes in the shared-memory band
+    MC_SITE_COPY_OUT = 9,      // a band's bytes in the env's observation
+    MC_SITE_DEBUG = 10,        // per-pixel debug code
+    MC_SITE_PATCH = 11,        // the interaction's voxel patched into the staged world
+    MC_SITE_TABLE = 12,        // u/v tables, colour tables
+    MC_SITE_STAGE = 13,        // a bulk copy's destination vs the CTA's dynamic shared memory
+};
 
 // Polls of an mbarrier before a bulk-copy wait gives up (each poll is one
 // try_wait, which itself blocks for a short hardware-defined time).
@@ -148,6 +166,10 @@ struct mc_backend {
     // the team kernel over rk's groups: grid = SMs x ctas_per_sm (at most one unit per team)
     int (*step_team)(const mc_ragged_kp* rk, int family, int obs_f32, int warps_per_cta, int ctas_per_sm,
                      int num_sms, cudaStream_t s);
+    // debug build (MC_CHECK_BOUNDS=1): read and clear the bounds-check record; -1 in the normal build
+    int (*bounds_report)(int32_t out[4], cudaStream_t s);
+    // debug build: one failed check at site 0 with no access behind it; -1 in the normal build
+    int (*bounds_selftest)(cudaStream_t s);
 };
 
 extern "C" const mc_backend* mc_backend_fast();

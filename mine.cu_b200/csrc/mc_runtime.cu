@@ -23,6 +23,11 @@
 #include "mc_internal.h"
 #include "mc_philox.h"
 
+#ifndef MC_CHECK_BOUNDS
+#define MC_CHECK_BOUNDS 0
+#endif
+#define MC_CHECK_BOUNDS_BUILD MC_CHECK_BOUNDS
+
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
@@ -1088,6 +1093,25 @@ extern "C" int64_t mc_env_fused_smem_bytes(const mc_env* e) {
     return (int64_t)e->be->fused_smem_bytes(&k, &e->fcfg);
 }
 
+extern "C" int mc_debug_bounds_report(int32_t numerics, int32_t* out, void* stream) {
+    if (!out) return fail(MC_ERR_INVALID, "out is NULL");
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics %d", numerics);
+    const int rc = be->bounds_report(out, (cudaStream_t)stream);
+    if (rc < 0) return fail(MC_ERR_UNSUPPORTED, "not the bounds-checked build (libminecu_b200_checked.so)");
+    return backend_rc(rc, "bounds report");
+}
+
+extern "C" int mc_debug_bounds_selftest(int32_t numerics, void* stream) {
+    const mc_backend* be = backend_of(numerics);
+    if (!be) return fail(MC_ERR_INVALID, "unknown numerics %d", numerics);
+    const int rc = be->bounds_selftest((cudaStream_t)stream);
+    if (rc < 0) return fail(MC_ERR_UNSUPPORTED, "not the bounds-checked build (libminecu_b200_checked.so)");
+    return backend_rc(rc, "bounds self-test");
+}
+
+extern "C" int mc_build_checks_bounds(void) { return MC_CHECK_BOUNDS_BUILD; }
+
 extern "C" int mc_env_check_error(mc_env* e, void* stream) {
     if (!e) return fail(MC_ERR_INVALID, "env is NULL");
     int32_t h[MC_FLAG_WORDS];
@@ -1100,7 +1124,9 @@ extern "C" int mc_env_check_error(mc_env* e, void* stream) {
         MC_CK(cudaMemcpyAsync(e->flags + MC_FLAG_ERROR, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
         MC_CK(cudaStreamSynchronize(s));
         return fail(MC_ERR_KERNEL, "kernel error %d (%s)", code,
-                    code == MC_KERR_TMA_TIMEOUT ? "bulk copy wait timed out" : "unknown");
+                    code == MC_KERR_TMA_TIMEOUT ? "bulk copy wait timed out"
+                                                : (code == MC_KERR_BOUNDS ? "index out of bounds (debug build)"
+                                                                          : "unknown"));
     }
     return MC_OK;
 }

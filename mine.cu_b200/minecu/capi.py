@@ -15,6 +15,9 @@ from typing import List
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libminecu_b200.so")
+# the same library with every index bounds-checked (a debug build; see
+# mc_build_checks_bounds in the header)
+CHECKED_LIB_PATH = os.path.join(_HERE, "libminecu_b200_checked.so")
 HEADER = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "minecu_b200.h")
 
 MC_OK, MC_ERR_INVALID, MC_ERR_CUDA, MC_ERR_KERNEL, MC_ERR_UNSUPPORTED = 0, -1, -2, -3, -4
@@ -121,6 +124,9 @@ _PROTOS = {
     "mc_env_set_fused_config": (I, [P, ctypes.POINTER(FusedConfig)]),
     "mc_env_get_fused_config": (I, [P, ctypes.POINTER(FusedConfig)]),
     "mc_env_check_error": (I, [P, P]),
+    "mc_build_checks_bounds": (I, []),
+    "mc_debug_bounds_report": (I, [c_int32, P, P]),
+    "mc_debug_bounds_selftest": (I, [c_int32, P]),
     "mc_env_fused_smem_bytes": (ctypes.c_int64, [P]),
     "mc_default_fused_config": (I, [PCFG, c_int32, c_int32, P, P]),
     "mc_ragged_create": (I, [ctypes.POINTER(c_void_p), I, ctypes.POINTER(c_void_p)]),
@@ -164,18 +170,28 @@ _PROTOS = {
 }
 
 _lib = None
+_checked_lib = None
 
 
-def lib() -> ctypes.CDLL:
-    """Load libminecu_b200.so (raises OSError if it is not built)."""
-    global _lib
+def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+def lib(checked: bool = False) -> ctypes.CDLL:
+    """Load libminecu_b200.so, or with checked=True the bounds-checked debug
+    build libminecu_b200_checked.so (raises OSError if it is not built).
+    Both link with -Bsymbolic, so the two can be loaded in one process."""
+    global _lib, _checked_lib
+    if checked:
+        if _checked_lib is None:
+            _checked_lib = _bind(ctypes.CDLL(CHECKED_LIB_PATH, mode=ctypes.RTLD_LOCAL))
+        return _checked_lib
     if _lib is None:
-        L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
-        for name, (res, args) in _PROTOS.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = L
+        _lib = _bind(ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL))
     return _lib
 
 
@@ -186,13 +202,13 @@ def header_functions() -> List[str]:
     return sorted(set(re.findall(r"\b(mc_[a-z0-9_]+)\s*\(", src)))
 
 
-def last_error() -> str:
-    return lib().mc_last_error().decode(errors="replace")
+def last_error(L: ctypes.CDLL = None) -> str:
+    return (L or lib()).mc_last_error().decode(errors="replace")
 
 
-def check(rc: int, what: str = "call") -> None:
+def check(rc: int, what: str = "call", L: ctypes.CDLL = None) -> None:
     if rc != MC_OK:
-        raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
+        raise RuntimeError(f"{what} failed ({rc}): {last_error(L)}")
 
 
 def make_config(batch_size, world_x, world_y, world_z, render_width, render_height, obs_dtype="uint8",

@@ -18,9 +18,11 @@ class GpuEnv:
     """An mc_env over torch-allocated state, driven through the C-ABI."""
 
     def __init__(self, device, batch_size, world_size=16, world_x=None, world_y=None, world_z=None,
-                 render_width=32, render_height=32, obs_dtype="uint8", numerics="ieee", debug=True, **kw):
+                 render_width=32, render_height=32, obs_dtype="uint8", numerics="ieee", debug=True, checked=False,
+                 **kw):
         import torch
         self.torch = torch
+        self.L = capi.lib(checked=checked)  # checked: the bounds-checked debug build
         self.B = batch_size
         self.wx = world_x or world_size
         self.wy = world_y or world_size
@@ -45,16 +47,16 @@ class GpuEnv:
         for k, v in self.t.items():
             setattr(self.st, k, None if v is None or v.numel() == 0 else v.data_ptr())
         self.h = ctypes.c_void_p()
-        capi.check(capi.lib().mc_env_create(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.h)),
-                   "mc_env_create")
+        capi.check(self.L.mc_env_create(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.h)),
+                   "mc_env_create", L=self.L)
         self.buttons = z(B, 8, dt=torch.int8)
         self.look = z(B, 2)
         self.actions = z(B, dt=torch.uint8)
-        capi.check(capi.lib().mc_env_generate_world(self.h, None), "generate_world")
+        capi.check(self.L.mc_env_generate_world(self.h, None), "generate_world", L=self.L)
 
     def close(self):
         if self.h:
-            capi.lib().mc_env_destroy(self.h)
+            self.L.mc_env_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):
@@ -64,37 +66,37 @@ class GpuEnv:
             pass
 
     def set_regen(self, per_env: bool):
-        capi.check(capi.lib().mc_env_set_regen_mode(self.h, 1 if per_env else 0), "set_regen_mode")
-        assert capi.lib().mc_env_get_regen_mode(self.h) == (1 if per_env else 0)
+        capi.check(self.L.mc_env_set_regen_mode(self.h, 1 if per_env else 0), "set_regen_mode", L=self.L)
+        assert self.L.mc_env_get_regen_mode(self.h) == (1 if per_env else 0)
 
     def set_fused(self, stage, warps_per_cta=8, ctas_per_sm=4, tile_w=8, team_warps=1, coop=0):
         f = capi.FusedConfig(stage, warps_per_cta, ctas_per_sm, tile_w, team_warps, coop)
-        capi.check(capi.lib().mc_env_set_fused_config(self.h, ctypes.byref(f)), "set_fused_config")
+        capi.check(self.L.mc_env_set_fused_config(self.h, ctypes.byref(f)), "set_fused_config", L=self.L)
 
     def reset(self, mask: Optional[np.ndarray] = None):
         m = None
         if mask is not None:
             m = self.torch.as_tensor(mask.astype(bool), device=self.t["voxels"].device)
-        capi.check(capi.lib().mc_env_reset(self.h, None if m is None else m.data_ptr(), None), "reset")
+        capi.check(self.L.mc_env_reset(self.h, None if m is None else m.data_ptr(), None), "reset", L=self.L)
         self.torch.cuda.synchronize()
 
     def step(self, buttons: np.ndarray, look: np.ndarray, form: int):
         self.buttons.copy_(self.torch.from_numpy(np.ascontiguousarray(buttons, np.int8)))
         self.look.copy_(self.torch.from_numpy(np.ascontiguousarray(look, np.float32)))
-        capi.check(capi.lib().mc_env_step(self.h, self.buttons.data_ptr(), self.look.data_ptr(), form, None), "step")
+        capi.check(self.L.mc_env_step(self.h, self.buttons.data_ptr(), self.look.data_ptr(), form, None), "step", L=self.L)
         self.torch.cuda.synchronize()
 
     def step_discrete(self, actions: np.ndarray, form: int):
         self.actions.copy_(self.torch.from_numpy(np.ascontiguousarray(actions, np.uint8)))
-        capi.check(capi.lib().mc_env_step_discrete(self.h, self.actions.data_ptr(), form, None), "step")
+        capi.check(self.L.mc_env_step_discrete(self.h, self.actions.data_ptr(), form, None), "step", L=self.L)
         self.torch.cuda.synchronize()
 
     def render(self):
-        capi.check(capi.lib().mc_env_render(self.h, None), "render")
+        capi.check(self.L.mc_env_render(self.h, None), "render", L=self.L)
         self.torch.cuda.synchronize()
 
     def check_error(self):
-        capi.check(capi.lib().mc_env_check_error(self.h, None), "check_error")
+        capi.check(self.L.mc_env_check_error(self.h, None), "check_error", L=self.L)
 
     def state(self) -> Dict[str, np.ndarray]:
         out = {}

@@ -136,3 +136,24 @@ def test_default_launch_shape_choices():
     assert f.coop == 1  # the one-warp band does not fit: team shape
     f, _ = _default_shape(32768, 32, 32, 16, "uint8", aligned=0)
     assert f.stage == 0  # bulk copies need 16-byte aligned worlds
+
+
+def test_normal_build_checks_no_bounds():
+    L = capi.lib()
+    assert L.mc_build_checks_bounds() == 0
+    out = (ctypes.c_int32 * 4)()
+    assert L.mc_debug_bounds_report(capi.NUMERICS_IEEE, out, None) == capi.MC_ERR_UNSUPPORTED
+    assert L.mc_debug_bounds_selftest(capi.NUMERICS_IEEE, None) == capi.MC_ERR_UNSUPPORTED
+
+
+def test_checked_build_loads_beside_the_normal_one():
+    """The bounds-checked debug build exports the same functions and says it
+    checks; loading it does not change which build the normal handle calls."""
+    import os
+    if not os.path.exists(capi.CHECKED_LIB_PATH):
+        pytest.skip("debug build not built")
+    C = capi.lib(checked=True)
+    missing = [n for n in capi.header_functions() if not hasattr(C, n)]
+    assert not missing, missing
+    assert C.mc_build_checks_bounds() == 1
+    assert capi.lib().mc_build_checks_bounds() == 0
