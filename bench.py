@@ -702,7 +702,8 @@ def run_reference(args):
         "unit": "env-steps/s", "n_gpus": 1, "steps": Kr,
         "warmup": Wm, "ms_per_step": t / Kr * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference world generator, Philox actions)",
-        "config": {"workload": W["workload"], "global_batch": B, "obs_dtype": W["obs_dtype"],
+        "config": {"workload": W["workload"], "global_batch": B, "world": "{0}x{0}x{0}".format(W["world"]),
+                   "render": "{0}x{0}x3 uint8".format(W["res"]), "obs_dtype": W["obs_dtype"],
                    "trajectory": f"steps {Wm}..{Wm + Kr - 1} after reset()",
                    "path": "reference src/kernels.cu launch_step_uint8 + MineEnv.step glue (eager, default stream)"},
         "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": B * 16, "d2h_bytes_per_step": B * 5},
