@@ -114,6 +114,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+CLOCK_HOLD_S = 0.6
+
+
+def hold_load(fn, seconds):
+    """Replay fn (one timed region's work) for about `seconds`, so that the
+    clock sampler sees the GPU under the same load as the timed region."""
+    import torch
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        fn()
+        torch.cuda.synchronize()
+
+
 def dist_setup(n_gpus):
     import torch
     import torch.distributed as dist
@@ -245,6 +258,9 @@ def run_mine(args):
     start()
     with ClockSampler(local) as clk:
         t_fused = timed(lambda: env.rollout(acts_t))
+        # a short timed region sees few nvidia-smi samples: keep the same
+        # load running under the sampler for a while (not part of the value)
+        hold_load(lambda: env.rollout(acts_t), CLOCK_HOLD_S)
     env.check_error()
     value = B * K * world / t_fused
 
@@ -363,6 +379,10 @@ def run_mine(args):
             modes[mode] = {"value": B * K * world / t_m, "ms_per_step": t_m / K * 1e3}
             del env_m
 
+    legs = None
+    if args.workload == "peak" and not args.shape and saved is None and world == 1 and not args.no_legs:
+        legs = mine_legs(args, dev, env, W)
+
     peak, peak_kind = load_peaks()
     achieved = bytes_per_env_step * B / (t_fused / K) / 1e9
     line = {
@@ -404,6 +424,9 @@ def run_mine(args):
         line["modes"] = modes
     if policy is not None:
         line["policy_obs"] = policy
+    if legs is not None:
+        line["workloads"] = legs
+        line["late_window"] = legs["late_window"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B=min(2048, B // 2) if B > 1 else 1, W=W)
     if rank == 0:
@@ -619,6 +642,201 @@ def run_mine_ragged(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Workload legs of the default run: the late trajectory window of the peak
+# shape, and the render-dominated, ragged and serving workloads, so that one
+# `python bench.py` (and one `--impl reference`) measures all of them.
+# ---------------------------------------------------------------------------
+LATE_START = 700  # first timed step of the late window (most cameras have dug in by then)
+LEG_STEPS = 50    # timed steps of the render and ragged legs
+SERVE_LEG_LOADS = (0.8, 0.85)
+SERVE_LEG_SECONDS = 1.0
+
+
+def _event_time(fn):
+    import torch
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def _roof(bytes_per_step, seconds_per_step):
+    peak, kind = load_peaks()
+    a = bytes_per_step / seconds_per_step / 1e9
+    return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak, "peak_kind": kind}
+
+
+def mine_legs(args, dev, env, W):
+    """This build's legs (see above); `env` is the peak-shape env."""
+    import torch
+    from minecu import MineEnv, _C, autotune
+    from minecu.ragged import RaggedBatch
+    from minecu.server import EnvServer
+    K, B = args.steps, W["batch_size"]
+    legs = {}
+    # late window of the peak shape: steps LATE_START.. after reset(), fused graph
+    a0 = torch.empty((LATE_START, B), dtype=torch.uint8, device=dev)
+    a1 = torch.empty((K, B), dtype=torch.uint8, device=dev)
+    _C.philox_actions(a0, 0, 0, W["seed"], W["break_half"])
+    _C.philox_actions(a1, 0, LATE_START, W["seed"], W["break_half"])
+    env.reset()
+    env.rollout(a0)
+    env.prepare_rollout(a1)
+    t = _event_time(lambda: env.rollout(a1))
+    env.check_error()
+    bpe = W["world"] ** 3 + W["res"] ** 2 * 3
+    legs["late_window"] = {"value": B * K / t, "unit": "env-steps/s", "ms_per_step": t / K * 1e3,
+                           "trajectory": f"steps {LATE_START}..{LATE_START + K - 1} after reset()",
+                           "roofline": _roof(bpe * B, t / K)}
+    del a0, a1
+    # render-dominated: B=4096, 32^3, 64x64, half break actions
+    R = RENDER_WORKLOAD
+    Wm = args.warmup
+    er = MineEnv(batch_size=R["batch_size"], world_size=R["world"], render_width=R["res"], render_height=R["res"],
+                 device=str(dev), max_steps=R["max_steps"], obs_dtype="uint8", look_delta=R["look_delta"])
+    aw = torch.empty((Wm, R["batch_size"]), dtype=torch.uint8, device=dev)
+    at = torch.empty((LEG_STEPS, R["batch_size"]), dtype=torch.uint8, device=dev)
+    _C.philox_actions(aw, 0, 0, R["seed"], True)
+    _C.philox_actions(at, 0, Wm, R["seed"], True)
+    er.reset()
+    er.rollout(aw)
+    er.prepare_rollout(at)
+    t = _event_time(lambda: er.rollout(at))
+    er.check_error()
+    er.form = "plain"
+    er.reset()
+    for s_ in range(Wm):
+        er.step(aw[s_])
+    tp = _event_time(lambda: [er.step(at[s_]) for s_ in range(LEG_STEPS)])
+    bpr = R["world"] ** 3 + R["res"] ** 2 * 3
+    legs["render"] = {"workload": R["workload"], "value": R["batch_size"] * LEG_STEPS / t, "unit": "env-steps/s",
+                      "ms_per_step": t / LEG_STEPS * 1e3, "plain_ms_per_step": tp / LEG_STEPS * 1e3,
+                      "launch": er.launch_config(), "trajectory": f"steps {Wm}..{Wm + LEG_STEPS - 1} after reset()",
+                      "roofline": _roof(bpr * R["batch_size"], t / LEG_STEPS)}
+    del er, aw, at
+    # ragged: 24,576 envs in 6 groups, autotuned (a short search), one launch per step
+    envs = [MineEnv(batch_size=b, world_size=w, render_width=r, render_height=r, device=str(dev),
+                    ground_height=ragged_ground(w), obs_dtype="uint8") for b, w, r in RAGGED_GROUPS]
+    batch = RaggedBatch(envs)
+    t_tune = time.perf_counter()
+    tuned = autotune.tune_ragged(batch, steps=10, warm_steps=20, rounds=1, use_cache=False)
+    t_tune = time.perf_counter() - t_tune
+    total = batch.total
+    aw = torch.empty((Wm, total), dtype=torch.uint8, device=dev)
+    at = torch.empty((LEG_STEPS, total), dtype=torch.uint8, device=dev)
+    _C.philox_actions(aw, 0, 0, RAGGED_SEED)
+    _C.philox_actions(at, 0, Wm, RAGGED_SEED)
+    batch.reset()
+    batch.rollout(aw)
+    batch.prepare_rollout(at)
+    t = _event_time(lambda: batch.rollout(at))
+    batch.check_error()
+    legs["ragged"] = {"workload": "ragged: 6 groups " + ", ".join(f"({b}, {w}^3, {r}x{r})" for b, w, r in
+                                                                 RAGGED_GROUPS),
+                      "value": total * LEG_STEPS / t, "unit": "env-steps/s", "ms_per_step": t / LEG_STEPS * 1e3,
+                      "launch": tuned["config"], "autotune": {"trials": tuned["trials"], "seconds": round(t_tune, 1)},
+                      "trajectory": f"steps {Wm}..{Wm + LEG_STEPS - 1} after reset()",
+                      "roofline": _roof(ragged_bytes_per_step(), t / LEG_STEPS)}
+    del batch, envs, aw, at
+    # serving: closed-loop peak, then Poisson arrivals at 80% and 85% of it
+    jobs = serve_jobs()
+    srv = EnvServer(hbm_budget_bytes=150e9, batching=True, max_inflight=2, max_envs_per_launch=16384, device=dev)
+    ids = [srv.admit(j["batch"], world_size=j["world"], render_width=j["res"], render_height=j["res"]) for j in jobs]
+    srv.drive([(i, 0.0, 0, k + 1) for k, i in enumerate(ids)], seconds=0.3, closed_loop=True)  # warm-up
+    pk = srv.drive([(i, 0.0, j["episode"], k + 1) for k, (i, j) in enumerate(zip(ids, jobs))],
+                   seconds=SERVE_LEG_SECONDS, closed_loop=True)
+    ntot = sum(j["batch"] for j in jobs)
+    loads = []
+    for frac in SERVE_LEG_LOADS:
+        st = srv.drive([(i, frac * pk["env_steps_per_s"] / ntot, j["episode"], k + 1)
+                        for k, (i, j) in enumerate(zip(ids, jobs))], seconds=SERVE_LEG_SECONDS)
+        loads.append({"offered_frac": frac, "env_steps_per_s": st["env_steps_per_s"], "p50_us": st["p50_us"],
+                      "p99_us": st["p99_us"], "max_us": st["max_us"]})
+    srv.close()
+    mean_bytes = sum(j["batch"] * (j["world"] ** 3 + j["res"] ** 2 * 3) for j in jobs) / ntot
+    legs["serve"] = {"workload": "16 jobs (batch 256..8192 log-uniform, 16^3 or 32^3, 32x32 or 64x64), Poisson "
+                                 "arrivals, HBM budget 150 GB",
+                     "closed_loop_env_steps_per_s": pk["env_steps_per_s"], "closed_loop_p99_us": pk["p99_us"],
+                     "loads": loads, "seconds_per_level": SERVE_LEG_SECONDS,
+                     "roofline_at_closed_loop": _roof(mean_bytes * pk["env_steps_per_s"], 1.0)}
+    return legs
+
+
+def reference_legs(args, dev, W):
+    """The reference build's legs: the late window of the peak shape and
+    the render-dominated and ragged workloads (it has no server)."""
+    import torch
+    import oracle as O
+    import ref_driver
+    K, B = args.steps, W["batch_size"]
+
+    def buttons(n, s0, steps, seed, break_half):
+        bt = torch.empty((steps, n, 8), dtype=torch.int8)
+        lk = torch.empty((steps, n, 2), dtype=torch.float32)
+        for s_ in range(steps):
+            b_, l_ = O.discrete_to_buttons(O.philox_actions(n, s0 + s_, seed, break_half=break_half), 0.1)
+            bt[s_] = torch.from_numpy(b_)
+            lk[s_] = torch.from_numpy(l_)
+        return bt.to(dev), lk.to(dev)
+
+    legs = {}
+    env = ref_driver.RefEnv(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"],
+                            device=str(dev), max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], target_block=3)
+    bw, lw = buttons(B, 0, LATE_START, W["seed"], W["break_half"])
+    bt, lt = buttons(B, LATE_START, K, W["seed"], W["break_half"])
+    env.reset()
+    for s_ in range(LATE_START):
+        env.step(bw[s_], lw[s_])
+    t = _event_time(lambda: [env.step(bt[s_], lt[s_]) for s_ in range(K)])
+    legs["late_window"] = {"value": B * K / t, "unit": "env-steps/s", "ms_per_step": t / K * 1e3,
+                           "trajectory": f"steps {LATE_START}..{LATE_START + K - 1} after reset()"}
+    del env, bw, lw, bt, lt
+    R = RENDER_WORKLOAD
+    Wm = args.warmup
+    env = ref_driver.RefEnv(batch_size=R["batch_size"], world_size=R["world"], render_width=R["res"],
+                            render_height=R["res"], device=str(dev), max_steps=R["max_steps"], obs_dtype="uint8",
+                            target_block=3)
+    bw, lw = buttons(R["batch_size"], 0, Wm, R["seed"], True)
+    bt, lt = buttons(R["batch_size"], Wm, LEG_STEPS, R["seed"], True)
+    env.reset()
+    for s_ in range(Wm):
+        env.step(bw[s_], lw[s_])
+    t = _event_time(lambda: [env.step(bt[s_], lt[s_]) for s_ in range(LEG_STEPS)])
+    legs["render"] = {"workload": R["workload"], "value": R["batch_size"] * LEG_STEPS / t, "unit": "env-steps/s",
+                      "ms_per_step": t / LEG_STEPS * 1e3,
+                      "trajectory": f"steps {Wm}..{Wm + LEG_STEPS - 1} after reset()"}
+    del env, bw, lw, bt, lt
+    envs = [ref_driver.RefEnv(batch_size=b, world_size=w, render_width=r, render_height=r, device=str(dev),
+                              ground_height=ragged_ground(w), obs_dtype="uint8", target_block=3)
+            for b, w, r in RAGGED_GROUPS]
+    total = sum(b for b, _, _ in RAGGED_GROUPS)
+    offs = [0]
+    for b, _, _ in RAGGED_GROUPS:
+        offs.append(offs[-1] + b)
+    bw, lw = buttons(total, 0, Wm, RAGGED_SEED, False)
+    bt, lt = buttons(total, Wm, LEG_STEPS, RAGGED_SEED, False)
+    gb = [(bw[:, offs[g]:offs[g + 1]].contiguous(), lw[:, offs[g]:offs[g + 1]].contiguous(),
+           bt[:, offs[g]:offs[g + 1]].contiguous(), lt[:, offs[g]:offs[g + 1]].contiguous())
+          for g in range(len(envs))]
+    for e in envs:
+        e.reset()
+    for s_ in range(Wm):
+        for g, e in enumerate(envs):
+            e.step(gb[g][0][s_], gb[g][1][s_])
+    t = _event_time(lambda: [e.step(gb[g][2][s_], gb[g][3][s_]) for s_ in range(LEG_STEPS)
+                             for g, e in enumerate(envs)])
+    legs["ragged"] = {"workload": "ragged: the same 6 groups, one reference MineEnv each, stepped in turn",
+                      "value": total * LEG_STEPS / t, "unit": "env-steps/s", "ms_per_step": t / LEG_STEPS * 1e3,
+                      "trajectory": f"steps {Wm}..{Wm + LEG_STEPS - 1} after reset()"}
+    legs["serve"] = {"unavailable": "the reference has no env server"}
+    return legs
+
+
 def run_reference(args):
     """The reference's own CUDA build (oracle/_ref/libminecu_ref.so, its
     src/kernels.cu compiled unmodified) driven in its MineEnv.step order, on
@@ -713,6 +931,11 @@ def run_reference(args):
     }
     if modes:
         line["modes"] = modes
+    if args.workload == "peak" and not args.shape and not args.no_legs:
+        del env
+        legs = reference_legs(args, dev, W)
+        line["workloads"] = legs
+        line["late_window"] = legs["late_window"]
     print(json.dumps(line), flush=True)
 
 
@@ -918,6 +1141,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds per offered-load level (serve)")
     ap.add_argument("--shape", default="", help="peak workload override B,W,R (batch, world edge, resolution)")
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default launch configuration")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="peak: skip the late-window, render, ragged and serve legs of the default run")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

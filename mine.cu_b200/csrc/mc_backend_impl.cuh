@@ -1635,6 +1635,12 @@ struct FusedLayout {
 
 __host__ __device__ inline int mc_align16(int x) { return (x + 15) & ~15; }
 
+// Tables of the per-warp kernel's common-case render loop, at the start of
+// its shared memory: per block and shade code the colour times the shade
+// (13 x 4 float4), then per block the flat colour packed as r | g << 8 | b << 16.
+constexpr int kShadeTableBytes = 13 * 4 * 16;
+constexpr int kFastTableBytes = kShadeTableBytes + 64;
+
 __host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int wxz, int obs_f32, int stage,
                                                    int tile_w) {
     FusedLayout L;
@@ -1645,7 +1651,7 @@ __host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int 
     L.stage_bytes = mc_align16(W * L.tile_h * 3 * (obs_f32 ? 4 : 1));
     L.world_bytes = stage ? mc_align16(wxyz) : 0;
     L.warp_bytes = 16 + 128 + L.stage_bytes + L.world_bytes;  // 16: mbarrier, 128: packed_start table
-    L.head_bytes = mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
+    L.head_bytes = kFastTableBytes + mc_align16((W + H) * 4 + 13 * 3 * 4 + 16 + 13 * 3 + 3);
     // the march reads up to wx*wz bytes on either side of a staged world:
     // keep that much allocated before the first world and after the last
     L.pad_bytes = stage ? mc_align16(wxz) : 0;
@@ -1827,6 +1833,113 @@ __device__ __forceinline__ int staged_top_layer(const int8_t* world, int wx, int
 // same kernel needed spill slots at its 64-register budget (4 CTAs of 8 warps
 // per SM) and ran 8% slower on B=32768, 16^3, 32x32, so it keeps its own
 // copy; the parity tests hold the two kernels to the same bits.
+template <bool F32>
+__host__ __device__ constexpr int bpp_of() { return 3 * (F32 ? 4 : 1); }
+
+// The per-warp kernel's render of one env in the common case: the world is
+// staged, every ray's packed march starts from the per-env table of the
+// eight sign combinations (so the eye is inside the box, its voxel holds
+// air, and for the shaded family the whole box lies within view distance),
+// no debug output is asked for, and the image is a whole number of
+// tile_w x (32/tile_w) tiles.  Every per-env fact is settled before the
+// loop, so the per-ray code has no branch but the march's: the same
+// operations in the same order as shade_ray / flat_ray and shade_rgb (the
+// bits are identical), with the shading done for every lane and the sky
+// colour selected afterwards, the colour times the face's shade read from
+// s_cs (built with the same N::mul), and the band addresses stepped
+// incrementally.  Writes the observation band by band (16-byte stores).
+template <int FAM, bool F32>
+__device__ __forceinline__ void render_env_fast(const Cam& c, const Dda0& d0, const int4* start, uint32_t base,
+                                                int wxz, int nvox, float vd, float rcp_vd, int W, int H, int TW,
+                                                int lane, const float* s_u, const float* s_v, const float4* s_cs,
+                                                const uint32_t* s_rgbp, uint8_t* stage, uint8_t* oenv) {
+    constexpr bool SHADED = FAM == MC_FAM_SHADED;
+    constexpr bool TRIG = FAM != MC_FAM_PREBASIS;
+    constexpr int bpp = bpp_of<F32>();
+    constexpr int m = F32 ? 0x1 : 0x3;  // sky_fused_mask of the float32 / uint8 shaded kernels
+    const float sky0 = 0.53f, sky1 = 0.81f, sky2 = 0.92f;  // SKY_COLOR (c_sky)
+    const int TH = 32 / TW;
+    const int lx = lane % TW, ly = lane / TW;
+    const SmemRange chk = staged_range(base, wxz, nvox);
+    const int band_bytes = W * TH * bpp;
+    for (int row0 = 0; row0 < H; row0 += TH) {
+        const float v = s_v[row0 + ly];
+        const float yraw = N::mad(v, c.uy, c.fy);
+        uint8_t* sp = stage + (ly * W + lx) * bpp;
+        for (int tx0 = 0; tx0 < W; tx0 += TW, sp += TW * bpp) {
+            const float u = s_u[tx0 + lx];
+            float x, y = yraw, z;
+            if (TRIG) {
+                x = N::mad(v, c.ux, N::mad(c.sy, c.cp, N::mul(u, c.rx)));
+                z = N::mad(v, c.uz, N::mad(c.cy, c.cp, N::mul(u, c.rz)));
+            } else {
+                x = N::mad(v, c.ux, N::mad(u, c.rx, c.fx));
+                z = N::mad(v, c.uz, N::mad(u, c.rz, c.fz));
+            }
+            if (SHADED) {
+                const float len = N::sqrt(len2(x, y, z));
+                const float rl = N::rcp_of(len);
+                x = N::div_r(x, len, rl);
+                y = N::div_r(y, len, rl);
+                z = N::div_r(z, len, rl);
+            } else {
+                const float rs = N::rsqrt(len2(x, y, z));
+                x = N::mul(x, rs);
+                y = N::mul(y, rs);
+                z = N::mul(z, rs);
+            }
+            const float ix = (x != 0.0f) ? N::div(1.0f, x) : 1e30f;
+            const float iy = (y != 0.0f) ? N::div(1.0f, y) : 1e30f;
+            const float iz = (z != 0.0f) ? N::div(1.0f, z) : 1e30f;
+            const bool xp = x >= 0.0f, yp = y >= 0.0f, zp = z >= 0.0f;
+            float tmx = N::mul(xp ? d0.nxp : d0.nxm, ix);
+            float tmy = N::mul(yp ? d0.nyp : d0.nym, iy);
+            float tmz = N::mul(zp ? d0.nzp : d0.nzm, iz);
+            const int4 e = start[(xp ? 1 : 0) | (yp ? 2 : 0) | (zp ? 4 : 0)];
+            const int b = march_packed_shared(base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, fabsf(ix), fabsf(iy),
+                                              fabsf(iz), chk);
+            if (SHADED) {
+                // the axis of the last step, chosen again from the same distances
+                const bool bx = tmx < tmy && tmx < tmz;
+                const bool by = !bx && tmy < tmz;
+                const float t = bx ? tmx : (by ? tmy : tmz);
+                const bool hit = b >= 0 && !(t >= vd);
+                const int code = bx ? 0 : (by ? (yp ? 3 : 2) : 1);
+                const float4 cs = s_cs[(b >= 0 ? b : 0) * 4 + code];
+                float fog = fminf(N::div_r(t, vd, rcp_vd), 1.0f);
+                fog = N::mul(fog, fog);
+                const float omf = N::sub(1.0f, fog);
+                const float c0 = (m & 1) ? N::mad(sky0, fog, N::mul(cs.x, omf)) : N::mad(cs.x, omf, N::mul(sky0, fog));
+                const float c1 = (m & 2) ? N::mad(sky1, fog, N::mul(cs.y, omf)) : N::mad(cs.y, omf, N::mul(sky1, fog));
+                const float c2 = (m & 4) ? N::mad(sky2, fog, N::mul(cs.z, omf)) : N::mad(cs.z, omf, N::mul(sky2, fog));
+                const float o0 = hit ? c0 : sky0, o1 = hit ? c1 : sky1, o2 = hit ? c2 : sky2;
+                if (F32) {
+                    float* sf = reinterpret_cast<float*>(sp);
+                    sf[0] = o0;
+                    sf[1] = o1;
+                    sf[2] = o2;
+                } else {
+                    sp[0] = (uint8_t)to_u8(o0);
+                    sp[1] = (uint8_t)to_u8(o1);
+                    sp[2] = (uint8_t)to_u8(o2);
+                }
+            } else {
+                // SKY_COLOR_U8 (135, 206, 235) packed
+                const uint32_t col = b >= 0 ? s_rgbp[b] : (135u | (206u << 8) | (235u << 16));
+                sp[0] = (uint8_t)col;
+                sp[1] = (uint8_t)(col >> 8);
+                sp[2] = (uint8_t)(col >> 16);
+            }
+        }
+        __syncwarp();
+        // copy the band (rows row0 .. row0+TH-1) out with 16-byte stores
+        const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+        uint4* d4 = reinterpret_cast<uint4*>(oenv + (long long)row0 * W * bpp);
+        for (int k = lane; k < (band_bytes >> 4); k += 32) d4[k] = s4[k];
+        __syncwarp();
+    }
+}
+
 // Per-env facts of a render (EnvRender::bits).
 enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
 
@@ -1855,7 +1968,18 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     FusedLayout L = fused_layout(W, H, wxyz, p.wx * p.wz, F32, STAGE, tile_w);
 
     // --- tables -------------------------------------------------------------
-    float* s_u = reinterpret_cast<float*>(smem);
+    float4* s_cs = reinterpret_cast<float4*>(smem);                      // [13][4]
+    uint32_t* s_rgbp = reinterpret_cast<uint32_t*>(smem + kShadeTableBytes);  // [13]
+    for (int k = threadIdx.x; k < 13 * 4; k += blockDim.x) {
+        // shade codes: 0 x face, 1 z face, 2 y face stepping down, 3 y face stepping up (shade_rgb)
+        const int blk = k >> 2, code = k & 3;
+        const float shade = code == 0 ? 0.8f : (code == 1 ? 0.9f : (code == 2 ? 0.6f : 1.0f));
+        s_cs[k] = make_float4(N::mul(c_rgb[blk][0], shade), N::mul(c_rgb[blk][1], shade),
+                              N::mul(c_rgb[blk][2], shade), 0.0f);
+    }
+    for (int k = threadIdx.x; k < 13; k += blockDim.x)
+        s_rgbp[k] = (uint32_t)c_rgb8[k][0] | ((uint32_t)c_rgb8[k][1] << 8) | ((uint32_t)c_rgb8[k][2] << 16);
+    float* s_u = reinterpret_cast<float*>(smem + kFastTableBytes);
     float* s_v = s_u + W;
     float (*s_rgb)[3] = reinterpret_cast<float (*)[3]>(s_v + H);
     float* s_sky = reinterpret_cast<float*>(s_rgb + 13);
@@ -2086,6 +2210,16 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
             start = sstart;
         }
         const int TW = L.tile_w, TH = L.tile_h;
+        if constexpr (STAGE && (FAM == MC_FAM_SHADED || FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS)) {
+            // the common case: every ray takes the packed march over the staged
+            // world from the start-value table, no debug output, the image a
+            // whole number of tiles and bands that copy out in 16-byte pieces
+            if (start && !p.dbg_pixel && W % TW == 0 && H % TH == 0 && vec_ok && ((W * TH * bpp_of<F32>()) & 15) == 0) {
+                render_env_fast<FAM, F32>(c, d0, start, smem_u32(sworld), p.wx * p.wz, wxyz, p.vd, rcp_vd, W, H, TW,
+                                          lane, s_u, s_v, s_cs, s_rgbp, stage, oenv);
+                continue;
+            }
+        }
         const int lx = lane % TW, ly = lane / TW;
         const int bpp = 3 * (F32 ? 4 : 1);  // bytes per pixel
         for (int row0 = 0; row0 < H; row0 += TH) {
