@@ -2798,6 +2798,201 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
 }
 
 // ---------------------------------------------------------------------------
+// Team kernel with staging depth 2
+// ---------------------------------------------------------------------------
+// The same work as k_step_team, pipelined one unit deep: each team holds two
+// claimed units.  Before a team renders unit k, the warp(s) that step unit
+// k+1 run its agent step and start its world's bulk copy into the second
+// world buffer (and the second mbarrier) of their slot, so the copy and the
+// agent step overlap the render of unit k; the copy is waited for only when
+// unit k+1 is rendered.  The env's render constants wait in a per-warp
+// shared-memory stash between the two.
+static_assert(sizeof(EnvRender) <= MC_ENV_STASH_BYTES, "env stash");
+
+template <int FAM, bool F32>
+__global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __grid_constant__ mc_ragged_kp rk) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int TWN = rk.team_warps;
+    const int team = warp / TWN, wt = warp % TWN;
+    const int teams_per_cta = nwarps / TWN;
+    const int G = rk.ngroups;
+    FusedCtx cx;
+    load_colour_tables(smem, cx);
+    float* tables = reinterpret_cast<float*>(smem + rk.tables_off);
+    for (int g = 0; g < G; ++g)
+        build_uv_tables<FAM>(rk.groups[g], tables + rk.uv_off[g], tables + rk.uv_off[g] + rk.groups[g].W);
+    TeamShared* ts = reinterpret_cast<TeamShared*>(smem + rk.teams_off + team * rk.team_bytes);
+    int8_t* tworld = reinterpret_cast<int8_t*>(ts) + MC_TEAM_HEAD_BYTES;
+    uint8_t* wbase = smem + rk.warps_off + warp * rk.warp_bytes;
+    const uint32_t mbar0 = smem_u32(wbase);  // depth slot d's mbarrier at mbar0 + 8 d
+    EnvRender* stash = reinterpret_cast<EnvRender*>(wbase + 16);  // depth slot d's env at wbase + 16 + 96 d
+    cx.stage = wbase + 16 + 2 * MC_ENV_STASH_BYTES;
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const bool claimer = (wt == 0 && lane == 0);
+    const long long total_teams = (long long)gridDim.x * teams_per_cta;
+    const long long my_team = (long long)blockIdx.x * teams_per_cta + team;
+    const unsigned total_units = (unsigned)rk.ustart[G];
+    auto claim = [&](int k) -> unsigned {
+        if (rk.sched_dynamic) return atomicAdd(reinterpret_cast<unsigned*>(&rk.flags[MC_FLAG_WORK]), 1u);
+        const long long u = my_team + (long long)k * total_teams;
+        return u < (long long)total_units ? (unsigned)u : total_units;
+    };
+    if (claimer) {
+        ts->unit[0] = claim(0);
+        ts->unit[1] = claim(1);
+    }
+    __syncthreads();
+    const int bar = 1 + team, nthr = TWN * 32;
+    uint32_t phases = 0;          // bit d: parity of depth slot d's next wait
+    unsigned done_groups = 0;
+    bool warp_no_stage = false;   // a copy of this warp timed out: no more copies, render from global memory
+    uint32_t pending = 0;         // bit d: a timed-out copy into slot d may still be in flight
+    uint32_t pending_phases = 0;  // bit d: its parity
+
+    // Where unit u lies: its group, env, and whether this warp steps it.
+    struct Unit {
+        int g;
+        long long e;
+        bool coop, stepper;
+    };
+    auto locate = [&](unsigned u) -> Unit {
+        int vg = 0;
+        while (vg + 1 < G && (long long)u >= rk.ustart[vg + 1]) ++vg;
+        Unit t;
+        t.g = rk.order[vg];
+        const long long local = (long long)u - rk.ustart[vg];
+        t.coop = (rk.coop_mask >> t.g) & 1;
+        t.e = t.coop ? local : local * TWN + wt;
+        t.stepper = t.coop ? (wt == 0) : (t.e < rk.groups[t.g].B);
+        return t;
+    };
+    auto slot_world = [&](int d, bool coop) -> int8_t* {
+        return tworld + d * rk.world_stride + (coop ? 0 : wt * rk.slot_bytes);
+    };
+    // The stepper of unit u steps its env and starts its world's copy into depth slot d.
+    auto prepare = [&](unsigned u, int d) {
+        const Unit t = locate(u);
+        if (!t.stepper) return;
+        const mc_kp& p = rk.groups[t.g];
+        const int wxyz = p.wx * p.wy * p.wz;
+        const long long s0 = rk.start[t.g];
+        const ActionSrc act{rk.actions ? rk.actions + s0 : nullptr, rk.actions ? nullptr : rk.buttons + 8 * s0,
+                            rk.actions ? nullptr : rk.look + 2 * s0};
+        EnvRender r = agent_step<FAM>(p, act, t.e, lane);
+        if (lane == 0) {
+            if (r.bits & MC_ER_DONE) done_groups |= 1u << t.g;
+            if (rk.rewards_cat) {
+                rk.rewards_cat[s0 + t.e] = p.rewards[t.e];
+                rk.dones_cat[s0 + t.e] = (uint8_t)(r.bits & MC_ER_DONE);
+            }
+        }
+        bool staged = ((rk.stage_mask >> t.g) & 1) && !(r.bits & MC_ER_BURIED) && !warp_no_stage;
+        int8_t* world = slot_world(d, t.coop);
+#if MC_CHECK_BOUNDS
+        if (staged) {
+            const SmemRange dyn = dyn_smem_range();
+            const long long off = (long long)smem_u32(world) - dyn.lo;
+            if (!in_bounds(off, dyn.span, MC_SITE_STAGE) || !in_bounds(off + wxyz - 1, dyn.span, MC_SITE_STAGE))
+                staged = false;  // no copy issued: render from global memory
+        }
+#endif
+        if (staged && lane == 0) {
+            const uint32_t mb = mbar0 + 8 * d;
+            // generic-proxy reads of the slot's previous world must precede the copy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(wxyz) : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(world)),
+                "l"(p.voxels + t.e * (long long)wxyz), "r"(wxyz), "r"(mb)
+                : "memory");
+        }
+        r.bits |= staged ? MC_ER_STAGED : 0;
+        if (lane == 0) stash[d] = r;
+        __syncwarp();
+    };
+    // The stepper of unit u (slot d): wait for the world, patch and measure it.
+    auto finish = [&](const Unit& t, int d) {
+        const mc_kp& p = rk.groups[t.g];
+        const int wxyz = p.wx * p.wy * p.wz;
+        EnvRender r = stash[d];
+        if (r.bits & MC_ER_STAGED) {
+            int8_t* world = slot_world(d, t.coop);
+            const uint32_t ph = (phases >> d) & 1u;
+            if (mbar_wait(mbar0 + 8 * d, ph, p.wait_polls)) {
+                // the interaction may have written after the copy read the byte
+                if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
+                    world[r.mod_idx] = (int8_t)r.mod_val;
+                __syncwarp();
+                r.ytop = staged_top_layer(world, p.wx, p.wy, p.wz, lane);
+            } else {
+                if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
+                warp_no_stage = true;  // the copy may still land: render from global memory from now on
+                pending |= 1u << d;
+                pending_phases = (pending_phases & ~(1u << d)) | (ph << d);
+                r.bits &= ~MC_ER_STAGED;
+            }
+            phases ^= 1u << d;
+        }
+        if (lane == 0) {
+            if (t.coop) {
+                ts->r = r;
+                ts->band_ctr = 0;
+            } else {
+                stash[d] = r;
+            }
+        }
+        __syncwarp();
+    };
+
+    if (ts->unit[0] < total_units) prepare(ts->unit[0], 0);
+    for (int k = 0;; ++k) {
+        const int d = k & 1;
+        const unsigned u = ts->unit[d];
+        if (u >= total_units) break;
+        const Unit t = locate(u);
+        if (t.stepper) finish(t, d);
+        if (t.coop) team_sync(bar, nthr);
+        // step the next unit and start its copy, then render this one
+        const unsigned u1 = ts->unit[d ^ 1];
+        if (u1 < total_units) prepare(u1, d ^ 1);
+        const mc_kp& p = rk.groups[t.g];
+        if (t.coop || t.stepper) {
+            const EnvRender r = t.coop ? ts->r : stash[d];
+            cx.s_u = tables + rk.uv_off[t.g];
+            cx.s_v = cx.s_u + p.W;
+            cx.rcp_vd = N::rcp_of(p.vd);
+            const bool staged = (r.bits & MC_ER_STAGED) != 0;
+            const int8_t* gw = p.voxels + t.e * (long long)p.wx * p.wy * p.wz;
+            if (r.bits & MC_ER_BURIED)
+                fill_env<FAM, F32>(p, t.e, r, cx, t.coop ? wt * 32 + lane : lane, t.coop ? nthr : 32);
+            else
+                render_env<FAM, F32>(p, t.e, r, cx, VoxEither{staged ? slot_world(d, t.coop) : gw, staged},
+                                     rk.tile_w[t.g], lane, t.coop ? &ts->band_ctr : nullptr);
+        }
+        if (claimer) ts->unit[d] = claim(k + 2);
+        team_sync(bar, nthr);
+    }
+    // timed-out copies may still be in flight: let them land (bounded)
+    // before this warp's part of shared memory can be released
+    for (int d = 0; d < 2; ++d)
+        if ((pending >> d) & 1u) mbar_wait(mbar0 + 8 * d, (pending_phases >> d) & 1u);
+    if (lane == 0) {
+        for (int g = 0; g < G; ++g) bounds_to_flags(rk.groups[g].flags);
+        for (int g = 0; g < G; ++g)
+            if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);
+    }
+    if (claimer && rk.sched_dynamic) finish_dynamic(rk.flags, total_teams);
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 static inline int grid_1d(long long n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -2880,13 +3075,14 @@ static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, 
 
 template <int FAM, bool F32>
 static int launch_team_t(const mc_ragged_kp* rk, int warps_per_cta, int ctas_per_sm, int num_sms, cudaStream_t s) {
-    auto kern = k_step_team<FAM, F32>;
+    const bool deep = rk->depth == 2;
+    auto kern = deep ? k_step_team2<FAM, F32> : k_step_team<FAM, F32>;
     size_t smem = (size_t)rk->warps_off + (size_t)warps_per_cta * rk->warp_bytes + (size_t)rk->tail_bytes;
-    static size_t attr_set = 0;
-    if (smem > 48 * 1024 && smem > attr_set) {
+    static size_t attr_set[2] = {0, 0};  // per kernel of this instantiation
+    if (smem > 48 * 1024 && smem > attr_set[deep]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
-        attr_set = smem;
+        attr_set[deep] = smem;
     }
     const int teams_per_cta = warps_per_cta / rk->team_warps;
     long long ctas_needed = (rk->ustart[rk->ngroups] + teams_per_cta - 1) / teams_per_cta;

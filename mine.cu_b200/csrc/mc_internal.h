@@ -117,6 +117,7 @@ struct mc_fused_cfg {
 enum { MC_MAX_GROUPS = 16 };
 enum { MC_COLOUR_TABLE_BYTES = 224 };  // shared colour tables of the fused kernels (16-aligned)
 enum { MC_TEAM_HEAD_BYTES = 128 };     // per-team shared words ahead of the team's world buffer
+enum { MC_ENV_STASH_BYTES = 96 };      // one env's render constants, kept in shared memory (depth 2)
 struct mc_ragged_kp {
     mc_kp groups[MC_MAX_GROUPS];    // the groups' parameter blocks (kernel parameter space)
     // optional: every env's reward and done flag also written at its global
@@ -142,9 +143,13 @@ struct mc_ragged_kp {
     int sched_dynamic;              // 1: teams claim units from flags[MC_FLAG_WORK]
     // shared-memory layout (bytes): colour tables at 0, then
     int tables_off, teams_off, warps_off;
-    int team_bytes;                 // MC_TEAM_HEAD_BYTES + the team's world buffer
+    int team_bytes;                 // MC_TEAM_HEAD_BYTES + max(depth, 1) x world_stride
     int slot_bytes;                 // world slot of one warp of a per-warp staged group
-    int warp_bytes;                 // 16 (mbarrier) + one band of observation bytes
+    int depth;                      // staging depth: 0 none, 1 one world buffer per stepper, 2 two (the
+                                    // next unit's world is copied while the current one renders)
+    int world_stride;               // bytes of one depth slot of a team's world region
+    int warp_bytes;                 // 16 (two mbarriers) [+ depth 2: two env stashes] + one band of
+                                    // observation bytes
     int tail_bytes;                 // allocated after the warps: the march may read one world layer past the last world
 };
 

@@ -460,7 +460,7 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
     rk->sched_dynamic = 1;
     const int bpp = 3 * (kps[0]->obs_f32 ? 4 : 1);
     long long start = 0;
-    int uv = 0, band = 16, coop_world = 0, slot = 0, pad = 0;
+    int uv = 0, band = 16, coop_world = 0, slot = 0, pad = 0, depth = 0;
     for (int g = 0; g < G; ++g) {
         const mc_kp& k = *kps[g];
         const long long wxyz = (long long)k.wx * k.wy * k.wz;
@@ -474,6 +474,7 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
         if (coop[g]) rk->coop_mask |= 1 << g;
         if (stage[g]) {
             rk->stage_mask |= 1 << g;
+            depth = std::max(depth, stage[g]);  // the launch stages every staged group at the largest depth asked
             pad = std::max(pad, align16i((long long)k.wx * k.wz));
             if (coop[g])
                 coop_world = std::max(coop_world, align16i(wxyz));
@@ -504,9 +505,11 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
     // staged world: worlds that follow one another are farther apart than
     // that, so only the first needs bytes before it and the last bytes after
     if (rk->teams_off + MC_TEAM_HEAD_BYTES < pad) rk->teams_off += align16i(pad - rk->teams_off - MC_TEAM_HEAD_BYTES);
-    rk->team_bytes = MC_TEAM_HEAD_BYTES + std::max(coop_world, team_warps * slot);
+    rk->depth = depth;
+    rk->world_stride = std::max(coop_world, team_warps * slot);
+    rk->team_bytes = MC_TEAM_HEAD_BYTES + std::max(depth, 1) * rk->world_stride;
     rk->warps_off = rk->teams_off + (warps_per_cta / team_warps) * rk->team_bytes;
-    rk->warp_bytes = 16 + band;
+    rk->warp_bytes = 16 + (depth == 2 ? 2 * MC_ENV_STASH_BYTES : 0) + band;
     const int after = warps_per_cta * rk->warp_bytes;
     rk->tail_bytes = after < pad ? pad - after : 0;
 }
@@ -526,8 +529,8 @@ int team_validate(const mc_kp* const* kps, int G, const int* stage, const int* t
         const int tw = tile_w[g];
         if (tw != 4 && tw != 8 && tw != 16 && tw != 32)
             return fail(MC_ERR_INVALID, "group %d: tile_w must be 4, 8, 16 or 32", g);
-        if ((stage[g] != 0 && stage[g] != 1) || (coop[g] != 0 && coop[g] != 1))
-            return fail(MC_ERR_INVALID, "group %d: stage and coop must be 0 or 1", g);
+        if (stage[g] < 0 || stage[g] > 2 || (coop[g] != 0 && coop[g] != 1))
+            return fail(MC_ERR_INVALID, "group %d: stage (staging depth) must be 0, 1 or 2 and coop 0 or 1", g);
         if (stage[g]) {
             const mc_kp& k = *kps[g];
             if (((long long)k.wx * k.wy * k.wz) & 15)
@@ -553,6 +556,8 @@ static int validate_fused_kp(const mc_env_config* cfg, const mc_kp* kp, const mc
                              f->ctas_per_sm);
     }
     if (f->team_warps != 1) return fail(MC_ERR_INVALID, "team_warps must be 1 without coop");
+    if (f->stage != 0 && f->stage != 1)
+        return fail(MC_ERR_INVALID, "one warp per env stages at depth 0 or 1 (depth 2 needs a team launch)");
     if (f->warps_per_cta != 4 && f->warps_per_cta != 8)
         return fail(MC_ERR_INVALID, "warps_per_cta must be 4 or 8");
     if (f->tile_w != 4 && f->tile_w != 8 && f->tile_w != 16 && f->tile_w != 32)

@@ -8,8 +8,10 @@ own envs:
 * ``tile_w``        pixel tile a warp marches per iteration, tile_w x
                     (32 / tile_w) rays (one ray per lane: rays per warp
                     iteration = 32, in rows of tile_w; 4, 8, 16 or 32);
-* ``stage``         bulk-copy each marched world into shared memory (0/1):
-                    the staging depth, one world buffer per env in flight;
+* ``stage``         staging depth of the worlds in shared memory: 0 none, 1
+                    one world buffer per stepping warp, 2 two (team launches:
+                    the next unit's world is copied while the current one
+                    renders);
 * ``team_warps``    warps per team (1, 2, 4, 8);
 * ``coop``          1: a team renders each env together (envs per CTA =
                     teams per CTA); 0: each warp its own env (envs per CTA =
@@ -106,7 +108,7 @@ def env_candidates() -> List[Tuple[int, int, int, int, int, int]]:
     """(stage, warps_per_cta, ctas_per_sm, tile_w, team_warps, coop) tried by tune_env."""
     per_warp = [(st, wpc, cps, tw, 1, 0) for st in (0, 1) for wpc in (4, 8) for cps in (2, 4, 8)
                 for tw in TILE_WIDTHS]
-    teams = [(st, 8, cps, tw, team, 1) for st in (0, 1) for cps in (2, 3, 4) for tw in TILE_WIDTHS
+    teams = [(st, 8, cps, tw, team, 1) for st in (0, 1, 2) for cps in (2, 3, 4) for tw in TILE_WIDTHS
              for team in (2, 4, 8)]
     return per_warp + teams
 
@@ -236,6 +238,10 @@ def tune_ragged(batch, steps: int = 30, warm_steps: int = 50, seed: int = 3, use
                             c = with_()
                             c["coop"][g], c["stage"][g], c["tile_w"][g] = co, st, tw
                             improved |= consider(c)
+            # staging depth of every staged group (the launch uses the largest)
+            staged = [1 if x else 0 for x in best_cfg["stage"]]
+            for depth in (1, 2):
+                improved |= consider(with_(stage=[depth * x for x in staged]))
             # launch shape
             for w2 in (4, 8):
                 if w2 % best_cfg["team_warps"]:

@@ -119,8 +119,11 @@ class RaggedBatch:
     def set_launch_config(self, warps_per_cta: int, ctas_per_sm: int, stage: Sequence[int],
                           tile_w: Sequence[int], team_warps: int = 1, coop: Optional[Sequence[int]] = None) -> None:
         """Launch shape (warps per CTA, CTAs per SM, warps per team) and, per
-        group, shared-memory staging (0/1), pixel-tile width and whether a
-        whole team renders each env (coop 1) or each warp its own (0)."""
+        group, shared-memory staging depth (0: none, 1: one world buffer per
+        stepping warp, 2: two, the next unit's world copied while the current
+        one renders; the launch stages every staged group at the largest depth
+        asked), pixel-tile width and whether a whole team renders each env
+        (coop 1) or each warp its own (0)."""
         coop = [0] * len(self.envs) if coop is None else coop
         _C.ragged_set_config(self._r, int(warps_per_cta), int(ctas_per_sm), int(team_warps),
                              [int(s) for s in stage], [int(t) for t in tile_w], [int(c) for c in coop])

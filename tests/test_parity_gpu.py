@@ -123,7 +123,8 @@ EARLY_EXIT_CASES = {
 
 @pytest.mark.parametrize("case", sorted(EARLY_EXIT_CASES))
 @pytest.mark.parametrize("mode", ["uint8", "uint8_minimal"])
-@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1)], ids=["per_warp", "team"])
+@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1), (2, 8, 2, 8, 4, 1)],
+                         ids=["per_warp", "team", "team_depth2"])
 def test_early_exit_march_vs_oracle(cuda, case, mode, cfg):
     """The fused kernels without debug outputs, where the march over a
     staged world ends rays early (left the box, above the highest solid

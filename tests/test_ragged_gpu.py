@@ -89,6 +89,11 @@ def test_ragged_equals_separate_fused_ref_fast(cuda, obs_dtype):
     (8, 3, [1, 1, 1, 1], [4, 8, 8, 8], 8, [0, 1, 1, 1]),
     (8, 2, [0, 0, 1, 1], [4, 4, 16, 4], 4, [1, 1, 1, 1]),
     (4, 4, [1, 1, 0, 1], [8, 4, 4, 16], 4, [1, 0, 0, 1]),
+    # staging depth 2: the next unit's world is copied while the current one renders
+    (8, 2, [2, 2, 2, 2], [4, 8, 8, 8], 4, [0, 1, 1, 1]),
+    (8, 2, [2, 0, 2, 2], [8, 4, 16, 8], 2, [0, 0, 1, 1]),
+    (4, 2, [2, 2, 0, 2], [4, 4, 8, 16], 1, [0, 0, 0, 0]),
+    (8, 1, [2, 2, 2, 2], [4, 8, 4, 8], 8, [1, 1, 1, 1]),
 ])
 def test_ragged_launch_configs_bit_exact(cuda, config):
     """Every launch shape, team shape, tile shape and staging choice gives the same bits."""
@@ -104,7 +109,8 @@ def test_ragged_teams_all_families(cuda, obs_dtype):
 
 
 @pytest.mark.parametrize("mode", ["uint8", "float32", "uint8_minimal", "uint8_prebasis_full"])
-@pytest.mark.parametrize("team", [(2, 1, 1, 4), (8, 1, 0, 8), (8, 0, 1, 16), (4, 1, 1, 32)])
+@pytest.mark.parametrize("team", [(2, 1, 1, 4), (8, 1, 0, 8), (8, 0, 1, 16), (4, 1, 1, 32), (4, 1, 2, 8),
+                                  (2, 0, 2, 4)])
 def test_env_team_form_equals_per_warp(cuda, mode, team):
     """MineEnv with the team kernel (teams_warps, coop, stage, tile_w) equals the per-warp kernel."""
     import torch
