@@ -408,8 +408,9 @@ typedef struct mc_decode_buffers {
  * every mode but prebasis_full, do_reset is an input and step_count is not
  * touched and may be NULL (their episode logic runs in Python,
  * minecu/__init__.py:363-366, 435-436); for prebasis_full the episode check
- * and counter update run in the step.  The plain form writes the decode buffers as the reference
- * does (dec must be non-NULL); the fused form keeps them in registers. */
+ * and counter update run in the step.  The plain form writes the decode
+ * buffers as the reference does (dec must be non-NULL); the fused form keeps
+ * them in registers. */
 int mc_step_stateless(const mc_env_config* cfg, const mc_env_state* state, const int8_t* buttons,
                       const float* look, const mc_decode_buffers* dec, int32_t form, void* stream);
 /* launch_physics (src/kernels.cu:2234-2250) from the 8 decode inputs */

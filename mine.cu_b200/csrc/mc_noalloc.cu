@@ -14,6 +14,8 @@
 // cudaGetSymbolAddress (with that device current); make that first call
 // before any stream capture.  The address is kept for the life of the
 // process, so cudaDeviceReset on a device while the library is loaded is
+// not supported (the kept address would no longer name the array).  The address is kept for the life of the
+// process, so cudaDeviceReset on a device while the library is loaded is
 // not supported (the kept address would no longer name the array).  Every
 // call shares the one array, so calls that overlap on the GPU (different
 // streams, or different host threads on the same device) race on it.
@@ -30,6 +32,8 @@ namespace {
 constexpr size_t kFlagBytes = 256;  // MC_FLAG_WORDS ints, padded to the array alignment
 constexpr size_t kPerEnv = 5 * sizeof(float) + 3;  // fwd, strafe, dyaw, dpitch, speed + jump, brk, place
 constexpr size_t kScratchBytes = kFlagBytes + ((size_t)MC_NOALLOC_MAX_ENVS * kPerEnv + 255) / 256 * 256;
+static_assert(kFlagBytes >= MC_FLAG_WORDS * sizeof(int32_t), "the flag words must fit in front of the scratch");
+static_assert(kFlagBytes % 16 == 0, "the decode arrays after the flag words stay 16-byte aligned");
 static_assert(kFlagBytes >= MC_FLAG_WORDS * sizeof(int32_t), "the flag words must fit in front of the scratch");
 static_assert(kFlagBytes % 16 == 0, "the decode arrays after the flag words stay 16-byte aligned");
 
