@@ -320,6 +320,13 @@ typedef struct mc_server_stats {
 int mc_server_create(const mc_server_config* cfg, mc_server** out);
 /* Stops the threads after the requests already queued have run. */
 int mc_server_destroy(mc_server* s);
+/* Step requests of one job a batching launch may run (1..8, default 1): a
+ * launch takes the oldest request of every job with work (round 0), then
+ * the next queued request of those jobs (round 1), and so on while the
+ * launch's envs stay within max_envs_per_launch; the rounds run one after
+ * another (a team launch each), so a burst of one job's requests waits for
+ * one launch instead of one launch per request.  No reference counterpart. */
+int mc_server_set_rounds(mc_server* s, int32_t rounds);
 /* Device bytes one job of this configuration is charged at admission. */
 int64_t mc_server_job_bytes(const mc_env_config* cfg);
 /* Allocate and generate a job's worlds and spawn its agents (as MineEnv(...)

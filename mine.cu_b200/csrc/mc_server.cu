@@ -91,6 +91,7 @@ struct Slot {
     uint8_t* h_res = nullptr;  // pinned: rewards (cap floats), then dones (cap bytes)
     uint8_t* d_res = nullptr;
     std::vector<Req*> reqs;
+    std::vector<int> round;       // round of each request (a job's r-th request of the launch runs in round r)
     std::vector<long long> offs;  // env offset of each step request in the launch
     long long total = 0;          // envs of the step launch: rewards at [0, 4 total), dones after them
     bool step_launch = false;
@@ -175,6 +176,7 @@ struct mc_server {
     int num_sms = 0;
     const mc_backend* be = nullptr;
     long long cap = 0;
+    int rounds = 1;  // step requests of one job per launch (mc_server_set_rounds)
     std::mutex mu;
     std::condition_variable cv_work, cv_done, cv_slot, cv_flight;
     std::vector<std::unique_ptr<Job>> jobs;
@@ -212,8 +214,14 @@ int free_slot(const mc_server* s) {
     return -1;
 }
 
-// Requests of the next launch (called with the lock held).
-std::vector<Req*> take_batch(mc_server* s) {
+// Requests of the next launch (called with the lock held), with the round
+// each runs in.  Round 0 takes the oldest request of every job with work (up
+// to 16 step requests of one render family, oldest first, within the env
+// cap); round r > 0 takes the next queued request of the jobs that had one in
+// round r - 1, while the envs of the whole launch stay within the cap.  A
+// burst of one job's requests so runs in one launch (its steps one after
+// another, a team launch per round) instead of one launch per request.
+std::vector<Req*> take_batch(mc_server* s, std::vector<int>* rounds) {
     std::vector<Job*> cand;
     for (auto& j : s->jobs)
         if (j->live && !j->queue.empty()) cand.push_back(j.get());
@@ -239,6 +247,40 @@ std::vector<Req*> take_batch(mc_server* s) {
             out.push_back(r);
         }
     }
+    rounds->assign(out.size(), 0);
+    if (s->cfg.batching && s->rounds > 1) {
+        long long envs = 0;
+        int fam = -1, f32 = -1;  // every round's team launch renders one family
+        for (Req* r : out)
+            if (r->kind == MC_REQ_STEP) {
+                envs += r->job->cfg.batch_size;
+                fam = family_of_mode(r->job->cfg.obs_mode);
+                f32 = r->job->cfg.obs_mode == MC_OBS_FLOAT32;
+            }
+        std::vector<Job*> prev;
+        for (Req* r : out) prev.push_back(r->job);
+        for (int rd = 1; rd < s->rounds && !prev.empty(); ++rd) {
+            std::vector<Job*> next;
+            int steps = 0;
+            for (Job* j : prev) {
+                if ((int)j->queue.size() <= rd) continue;
+                Req* r = j->queue[rd];
+                if (r->kind == MC_REQ_STEP) {
+                    const int jf = family_of_mode(j->cfg.obs_mode), jf32 = j->cfg.obs_mode == MC_OBS_FLOAT32;
+                    if (steps == MC_RAGGED_MAX_GROUPS || (fam >= 0 && (jf != fam || jf32 != f32))) continue;
+                    if (envs + j->cfg.batch_size > s->cap) continue;
+                    fam = jf;
+                    f32 = jf32;
+                    envs += j->cfg.batch_size;
+                    ++steps;
+                }
+                out.push_back(r);
+                rounds->push_back(rd);
+                next.push_back(j);
+            }
+            prev.swap(next);
+        }
+    }
     for (Req* r : out) {
         r->job->queue.pop_front();
         r->job->inflight++;
@@ -249,33 +291,64 @@ std::vector<Req*> take_batch(mc_server* s) {
 
 // Enqueue the device work of one launch on the server stream (no lock held;
 // the jobs of `reqs` cannot be released while they are in flight).
+int run_round(mc_server* s, Slot& sl, const std::vector<Req*>& reqs, const std::vector<size_t>& steps,
+              cudaStream_t st);
+
 int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
     cudaStream_t st = s->stream;
     sl.offs.assign(reqs.size(), -1);
     sl.step_launch = false;
     int rc = MC_OK;
-    for (Req* r : reqs)
-        if (r->kind == MC_REQ_RESET && rc == MC_OK) rc = mc_env_reset(r->job->env, nullptr, st);
+    int nrounds = 1;
+    for (int rd : sl.round) nrounds = std::max(nrounds, rd + 1);
+    // step requests round by round, each round's in launch order: their envs'
+    // actions and results are contiguous per round
     std::vector<size_t> steps;
-    for (size_t i = 0; i < reqs.size(); ++i)
-        if (reqs[i]->kind == MC_REQ_STEP) steps.push_back(i);
-    if (!steps.empty() && rc == MC_OK) {
+    std::vector<size_t> round_first(nrounds + 1, 0);
+    for (int rd = 0; rd < nrounds; ++rd) {
+        round_first[rd] = steps.size();
+        for (size_t i = 0; i < reqs.size(); ++i)
+            if (sl.round[i] == rd && reqs[i]->kind == MC_REQ_STEP) steps.push_back(i);
+    }
+    round_first[nrounds] = steps.size();
+    long long off = 0;
+    for (size_t i : steps) {
+        Req* r = reqs[i];
+        memcpy(sl.h_act + off, r->actions.data(), r->actions.size());
+        sl.offs[i] = off;
+        off += r->job->cfg.batch_size;
+    }
+    sl.total = off;
+    if (!steps.empty()) {
         sl.step_launch = true;
-        long long off = 0;
-        for (size_t i : steps) {
-            Req* r = reqs[i];
-            memcpy(sl.h_act + off, r->actions.data(), r->actions.size());
-            sl.offs[i] = off;
-            off += r->job->cfg.batch_size;
-        }
         cudaError_t ce = cudaMemcpyAsync(sl.d_act, sl.h_act, (size_t)off, cudaMemcpyHostToDevice, s->up);
         if (ce == cudaSuccess) ce = cudaEventRecord(sl.ev_up, s->up);
         if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, sl.ev_up, 0);
         if (ce != cudaSuccess) return mc_cuda_fail(ce, "server: actions upload");
-        // rewards then dones, contiguous: one read-back
-        sl.total = off;
-        float* d_rew = reinterpret_cast<float*>(sl.d_res);
-        uint8_t* d_done = sl.d_res + off * 4;
+    }
+    for (int rd = 0; rd < nrounds && rc == MC_OK; ++rd) {
+        for (size_t i = 0; i < reqs.size(); ++i)
+            if (sl.round[i] == rd && reqs[i]->kind == MC_REQ_RESET && rc == MC_OK)
+                rc = mc_env_reset(reqs[i]->job->env, nullptr, st);
+        if (rc != MC_OK || round_first[rd] == round_first[rd + 1]) continue;
+        const std::vector<size_t> rsteps(steps.begin() + round_first[rd], steps.begin() + round_first[rd + 1]);
+        rc = run_round(s, sl, reqs, rsteps, st);
+    }
+    return rc;
+}
+
+// One round's step requests (at most one per job, one render family) as one
+// team launch plus the conditional regenerations.
+int run_round(mc_server* s, Slot& sl, const std::vector<Req*>& reqs, const std::vector<size_t>& steps,
+              cudaStream_t st) {
+    int rc = MC_OK;
+    cudaError_t ce = cudaSuccess;
+    {
+        const long long first = sl.offs[steps[0]];
+        // rewards then dones, contiguous over the launch: one read-back
+        float* d_rew = reinterpret_cast<float*>(sl.d_res) + first;
+        uint8_t* d_done = sl.d_res + sl.total * 4 + first;
+        uint8_t* d_act = sl.d_act + first;
         if (s->cfg.batching) {
             const int G = (int)steps.size();
             std::vector<const mc_kp*> kps(G);
@@ -295,7 +368,7 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
             mc_ragged_kp rk;
             team_layout(kps.data(), G, stage, tile_w, coop, team, 8, &rk);
             rk.flags = s->flags;
-            rk.actions = sl.d_act;
+            rk.actions = d_act;
             rk.rewards_cat = d_rew;
             rk.dones_cat = d_done;
             const mc_kp& k0 = *kps[0];
@@ -308,7 +381,7 @@ int run_batch(mc_server* s, Slot& sl, const std::vector<Req*>& reqs) {
                 }
         } else {
             Req* r = reqs[steps[0]];
-            rc = mc_env_step_discrete(r->job->env, sl.d_act, MC_FORM_PLAIN, st);
+            rc = mc_env_step_discrete(r->job->env, d_act, MC_FORM_PLAIN, st);
             if (rc) return rc;
             const long long B = r->job->cfg.batch_size;
             ce = cudaMemcpyAsync(d_rew, r->job->st.rewards, B * 4, cudaMemcpyDeviceToDevice, st);
@@ -353,7 +426,7 @@ void launcher_main(mc_server* s) {
             s->cv_slot.wait(lk, [&] { return free_slot(s) >= 0; });
             si = free_slot(s);
             s->slots[si].busy = true;
-            reqs = take_batch(s);
+            reqs = take_batch(s, &s->slots[si].round);
         }
         Slot& sl = s->slots[si];
         NvtxRange nvtx("mc_server launch");
@@ -552,6 +625,14 @@ extern "C" int mc_server_create(const mc_server_config* cfg, mc_server** out) {
     s->launcher = std::thread(launcher_main, s);
     s->completer = std::thread(completer_main, s);
     *out = s;
+    return MC_OK;
+}
+
+extern "C" int mc_server_set_rounds(mc_server* s, int32_t rounds) {
+    if (!s) return mc_fail(MC_ERR_INVALID, "server is NULL");
+    if (rounds < 1 || rounds > 8) return mc_fail(MC_ERR_INVALID, "rounds must be 1..8");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->rounds = rounds;
     return MC_OK;
 }
 

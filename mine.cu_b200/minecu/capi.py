@@ -144,6 +144,7 @@ _PROTOS = {
     "mc_ragged_check_error": (I, [P, P]),
     "mc_server_create": (I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(c_void_p)]),
     "mc_server_destroy": (I, [P]),
+    "mc_server_set_rounds": (I, [P, c_int32]),
     "mc_server_job_bytes": (ctypes.c_int64, [PCFG]),
     "mc_server_admit": (I, [P, PCFG, ctypes.POINTER(c_int32)]),
     "mc_server_release": (I, [P, I]),

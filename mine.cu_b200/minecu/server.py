@@ -40,7 +40,8 @@ class _DeviceArray:
 
 class EnvServer:
     def __init__(self, hbm_budget_bytes: float = 150e9, numerics: str = "ref_fast", batching: bool = True,
-                 max_inflight: int = 2, max_envs_per_launch: int = 0, device: Optional[torch.device] = None):
+                 max_inflight: int = 2, max_envs_per_launch: int = 0, device: Optional[torch.device] = None,
+                 rounds: int = 1):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.numerics = numerics
         self._L = capi.lib()
@@ -51,8 +52,16 @@ class EnvServer:
         with torch.cuda.device(self.device):
             torch.cuda.init()
             capi.check(self._L.mc_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "mc_server_create")
+        if rounds != 1:
+            self.set_rounds(rounds)
         self._jobs: Dict[int, capi.EnvConfig] = {}
         self._tickets: Dict[int, int] = {}  # ticket -> batch size of its results
+
+    def set_rounds(self, rounds: int) -> None:
+        """Step requests of one job a batching launch may run, one round
+        after another (1..8): a burst of a job's requests then waits for one
+        launch instead of one launch per request."""
+        capi.check(self._L.mc_server_set_rounds(self._h, int(rounds)), "mc_server_set_rounds")
 
     # ------------------------------------------------------------------
     def _config(self, batch_size: int, world_size: int = 16, render_width: int = 32, render_height: int = 32,

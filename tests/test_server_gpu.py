@@ -167,3 +167,49 @@ def test_server_threads_and_load_generator(cuda):
     closed = srv.drive([(j, 0.0, 0, j + 1) for j in jobs], seconds=0.5, closed_loop=True)
     assert closed["env_steps_per_s"] > 0 and closed["reset_requests"] == 0
     srv.close()
+
+
+def test_server_rounds_run_a_burst_in_one_launch(cuda):
+    """With rounds, a burst of one job's queued requests runs in one launch,
+    one round after another: every step's rewards and dones, and each job's
+    state afterwards, equal MineEnv stepping the same actions in order (a
+    reset request in the middle of a burst included)."""
+    import torch
+    from minecu.server import EnvServer
+    srv = EnvServer(hbm_budget_bytes=4e9, batching=True, rounds=4, max_inflight=1)
+    jobs = [_admit(srv, *j) for j in JOBS]
+    envs = [_env(cuda, *j) for j in JOBS]
+    for e in envs:
+        e.reset()
+    rng = np.random.default_rng(11)
+    for burst in range(4):
+        plan = []  # per job: list of ("step", actions) / ("reset", None)
+        for g, j in enumerate(JOBS):
+            reqs = [("step", rng.integers(0, 11, j[0], dtype=np.uint8)) for _ in range(3)]
+            if burst == 2 and g == 1:
+                reqs.insert(1, ("reset", None))
+            plan.append(reqs)
+        tickets = []
+        for g, reqs in enumerate(plan):  # every request queued before any runs finishes
+            tickets.append([srv.submit(jobs[g], a) if kind == "step" else srv.submit(jobs[g], reset=True)
+                            for kind, a in reqs])
+        for g, (reqs, ts) in enumerate(zip(plan, tickets)):
+            for (kind, a), t in zip(reqs, ts):
+                if kind == "reset":
+                    srv.wait(t)
+                    envs[g].reset()
+                    continue
+                rew, done = srv.wait(t)
+                _, r_ref, d_ref = envs[g].step(torch.from_numpy(a).to(cuda))
+                assert np.array_equal(rew.view(np.int32), r_ref.cpu().numpy().view(np.int32)), f"burst {burst} job {g}"
+                assert np.array_equal(done, d_ref.cpu().numpy()), f"burst {burst} job {g}: dones"
+        torch.cuda.synchronize()
+        for g, (job, e) in enumerate(zip(jobs, envs)):
+            st = srv.state(job)
+            for k in KEYS:
+                assert torch.equal(_bits(torch, st[k]), _bits(torch, getattr(e, k))), f"burst {burst} job {g}: {k}"
+            assert torch.equal(st["obs"], e.obs_buffer), f"burst {burst} job {g}: obs"
+    st = srv.stats()
+    assert st["step_requests"] == 4 * 3 * len(JOBS)
+    assert st["launches"] < st["step_requests"] / len(JOBS)  # bursts ran in fewer launches than requests per job
+    srv.close()
