@@ -91,8 +91,8 @@ def test_ragged_equals_separate_fused_ref_fast(cuda, obs_dtype):
     (4, 4, [1, 1, 0, 1], [8, 4, 4, 16], 4, [1, 0, 0, 1]),
     # staging depth 2: the next unit's world is copied while the current one renders
     (8, 2, [2, 2, 2, 2], [4, 8, 8, 8], 4, [0, 1, 1, 1]),
-    (8, 2, [2, 0, 2, 2], [8, 4, 16, 8], 2, [0, 0, 1, 1]),
-    (4, 2, [2, 2, 0, 2], [4, 4, 8, 16], 1, [0, 0, 0, 0]),
+    (4, 2, [2, 0, 2, 2], [8, 4, 16, 8], 2, [0, 0, 1, 1]),
+    (4, 2, [2, 2, 0, 0], [4, 4, 8, 16], 1, [0, 0, 0, 0]),
     (8, 1, [2, 2, 2, 2], [4, 8, 4, 8], 8, [1, 1, 1, 1]),
 ])
 def test_ragged_launch_configs_bit_exact(cuda, config):
