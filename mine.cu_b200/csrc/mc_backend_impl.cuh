@@ -1639,7 +1639,8 @@ __host__ __device__ inline int mc_align16(int x) { return (x + 15) & ~15; }
 // its shared memory: per block and shade code the colour times the shade
 // (13 x 4 float4), then per block the flat colour packed as r | g << 8 | b << 16.
 constexpr int kShadeTableBytes = 13 * 4 * 16;
-constexpr int kFastTableBytes = kShadeTableBytes + 64;
+constexpr int kFastTableBytes = MC_FAST_TABLE_BYTES;
+static_assert(kFastTableBytes == kShadeTableBytes + 64, "fast tables");
 
 __host__ __device__ inline FusedLayout fused_layout(int W, int H, int wxyz, int wxz, int obs_f32, int stage,
                                                    int tile_w) {
@@ -1715,7 +1716,24 @@ struct FusedCtx {
     int8_t* sworld;              // staged world of this warp
     uint32_t mbar_a;             // mbarrier of this warp
     float rcp_vd;                // reciprocal of the env's view distance
+    const float4* s_cs;          // colour x shade table of the common-case loop (fast_band)
+    const uint32_t* s_rgbp;      // packed flat colours
+    int4* sstart;                // this warp's table of march start values (8 entries)
 };
+
+// The common-case loop's tables: colour x shade per block and shade code
+// (0 x face, 1 z face, 2 y face stepping down, 3 y face stepping up, as in
+// shade_rgb) and the flat colours packed r | g << 8 | b << 16.
+__device__ __forceinline__ void build_fast_tables(float4* s_cs, uint32_t* s_rgbp) {
+    for (int k = threadIdx.x; k < 13 * 4; k += blockDim.x) {
+        const int blk = k >> 2, code = k & 3;
+        const float shade = code == 0 ? 0.8f : (code == 1 ? 0.9f : (code == 2 ? 0.6f : 1.0f));
+        s_cs[k] = make_float4(N::mul(c_rgb[blk][0], shade), N::mul(c_rgb[blk][1], shade),
+                              N::mul(c_rgb[blk][2], shade), 0.0f);
+    }
+    for (int k = threadIdx.x; k < 13; k += blockDim.x)
+        s_rgbp[k] = (uint32_t)c_rgb8[k][0] | ((uint32_t)c_rgb8[k][1] << 8) | ((uint32_t)c_rgb8[k][2] << 16);
+}
 
 // Shared colour tables: 13*3 + 4 floats, 13*3 + 3 bytes.
 constexpr int kColourTableBytes = 13 * 3 * 4 + 16 + 13 * 3 + 3;
@@ -1833,111 +1851,149 @@ __device__ __forceinline__ int staged_top_layer(const int8_t* world, int wx, int
 // same kernel needed spill slots at its 64-register budget (4 CTAs of 8 warps
 // per SM) and ran 8% slower on B=32768, 16^3, 32x32, so it keeps its own
 // copy; the parity tests hold the two kernels to the same bits.
-template <bool F32>
-__host__ __device__ constexpr int bpp_of() { return 3 * (F32 ? 4 : 1); }
+// The common-case render of one band of an env's image (both step
+// kernels): the world is staged, the eye is inside the box with air in its
+// voxel (every ray starts one DDA step in, and ends as sky when it leaves
+// the box), no debug output is asked for, and the image is a whole number of
+// tile_w x (32/tile_w) tiles.  Every ray's march start values come from a
+// per-env table of the eight ray sign combinations (packed_start for the
+// packed march, split_start for the split march).  Every per-env fact is
+// settled before the loop, so the per-ray code has no branch but the
+// march's: the same operations in the same order as shade_ray / flat_ray
+// and shade_rgb (the bits are identical), with the shading done for every
+// lane and the sky colour selected afterwards, the colour times the face's
+// shade read from s_cs (built with the same N::mul), and the band address
+// stepped incrementally.  The band goes to `stage`, then to `dst` with
+// 16-byte stores.
+struct FastEnv {
+    const int4* start;  // per sign combination: packed (index|counts, dx, dy, dz) or split (counts, dax, day, daz)
+    uint32_t base;      // staged world (packed) / the eye voxel's address in it (split)
+    SmemRange chk;      // the staged world +- one layer (debug build)
+    float vd, rcp_vd;
+};
 
-// The per-warp kernel's render of one env in the common case: the world is
-// staged, every ray's packed march starts from the per-env table of the
-// eight sign combinations (so the eye is inside the box, its voxel holds
-// air, and for the shaded family the whole box lies within view distance),
-// no debug output is asked for, and the image is a whole number of
-// tile_w x (32/tile_w) tiles.  Every per-env fact is settled before the
-// loop, so the per-ray code has no branch but the march's: the same
-// operations in the same order as shade_ray / flat_ray and shade_rgb (the
-// bits are identical), with the shading done for every lane and the sky
-// colour selected afterwards, the colour times the face's shade read from
-// s_cs (built with the same N::mul), and the band addresses stepped
-// incrementally.  Writes the observation band by band (16-byte stores).
-template <int FAM, bool F32>
-__device__ __forceinline__ void render_env_fast(const Cam& c, const Dda0& d0, const int4* start, uint32_t base,
-                                                int wxz, int nvox, float vd, float rcp_vd, int W, int H, int TW,
-                                                int lane, const float* s_u, const float* s_v, const float4* s_cs,
-                                                const uint32_t* s_rgbp, uint8_t* stage, uint8_t* oenv) {
+template <int FAM, bool F32, bool SPLIT>
+__device__ __forceinline__ void fast_band(const Cam& c, const Dda0& d0, const FastEnv& fe, int W, int TW, int row0,
+                                          int lane, const float* s_u, const float* s_v, const float4* s_cs,
+                                          const uint32_t* s_rgbp, uint8_t* stage, uint8_t* dst) {
     constexpr bool SHADED = FAM == MC_FAM_SHADED;
     constexpr bool TRIG = FAM != MC_FAM_PREBASIS;
-    constexpr int bpp = bpp_of<F32>();
+    constexpr int bpp = 3 * (F32 ? 4 : 1);
     constexpr int m = F32 ? 0x1 : 0x3;  // sky_fused_mask of the float32 / uint8 shaded kernels
     const float sky0 = 0.53f, sky1 = 0.81f, sky2 = 0.92f;  // SKY_COLOR (c_sky)
     const int TH = 32 / TW;
     const int lx = lane % TW, ly = lane / TW;
-    const SmemRange chk = staged_range(base, wxz, nvox);
-    const int band_bytes = W * TH * bpp;
-    for (int row0 = 0; row0 < H; row0 += TH) {
-        const float v = s_v[row0 + ly];
-        const float yraw = N::mad(v, c.uy, c.fy);
-        uint8_t* sp = stage + (ly * W + lx) * bpp;
-        for (int tx0 = 0; tx0 < W; tx0 += TW, sp += TW * bpp) {
-            const float u = s_u[tx0 + lx];
-            float x, y = yraw, z;
-            if (TRIG) {
-                x = N::mad(v, c.ux, N::mad(c.sy, c.cp, N::mul(u, c.rx)));
-                z = N::mad(v, c.uz, N::mad(c.cy, c.cp, N::mul(u, c.rz)));
-            } else {
-                x = N::mad(v, c.ux, N::mad(u, c.rx, c.fx));
-                z = N::mad(v, c.uz, N::mad(u, c.rz, c.fz));
-            }
-            if (SHADED) {
-                const float len = N::sqrt(len2(x, y, z));
-                const float rl = N::rcp_of(len);
-                x = N::div_r(x, len, rl);
-                y = N::div_r(y, len, rl);
-                z = N::div_r(z, len, rl);
-            } else {
-                const float rs = N::rsqrt(len2(x, y, z));
-                x = N::mul(x, rs);
-                y = N::mul(y, rs);
-                z = N::mul(z, rs);
-            }
-            const float ix = (x != 0.0f) ? N::div(1.0f, x) : 1e30f;
-            const float iy = (y != 0.0f) ? N::div(1.0f, y) : 1e30f;
-            const float iz = (z != 0.0f) ? N::div(1.0f, z) : 1e30f;
-            const bool xp = x >= 0.0f, yp = y >= 0.0f, zp = z >= 0.0f;
-            float tmx = N::mul(xp ? d0.nxp : d0.nxm, ix);
-            float tmy = N::mul(yp ? d0.nyp : d0.nym, iy);
-            float tmz = N::mul(zp ? d0.nzp : d0.nzm, iz);
-            const int4 e = start[(xp ? 1 : 0) | (yp ? 2 : 0) | (zp ? 4 : 0)];
-            const int b = march_packed_shared(base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, fabsf(ix), fabsf(iy),
-                                              fabsf(iz), chk);
-            if (SHADED) {
-                // the axis of the last step, chosen again from the same distances
-                const bool bx = tmx < tmy && tmx < tmz;
-                const bool by = !bx && tmy < tmz;
-                const float t = bx ? tmx : (by ? tmy : tmz);
-                const bool hit = b >= 0 && !(t >= vd);
-                const int code = bx ? 0 : (by ? (yp ? 3 : 2) : 1);
-                const float4 cs = s_cs[(b >= 0 ? b : 0) * 4 + code];
-                float fog = fminf(N::div_r(t, vd, rcp_vd), 1.0f);
-                fog = N::mul(fog, fog);
-                const float omf = N::sub(1.0f, fog);
-                const float c0 = (m & 1) ? N::mad(sky0, fog, N::mul(cs.x, omf)) : N::mad(cs.x, omf, N::mul(sky0, fog));
-                const float c1 = (m & 2) ? N::mad(sky1, fog, N::mul(cs.y, omf)) : N::mad(cs.y, omf, N::mul(sky1, fog));
-                const float c2 = (m & 4) ? N::mad(sky2, fog, N::mul(cs.z, omf)) : N::mad(cs.z, omf, N::mul(sky2, fog));
-                const float o0 = hit ? c0 : sky0, o1 = hit ? c1 : sky1, o2 = hit ? c2 : sky2;
-                if (F32) {
-                    float* sf = reinterpret_cast<float*>(sp);
-                    sf[0] = o0;
-                    sf[1] = o1;
-                    sf[2] = o2;
-                } else {
-                    sp[0] = (uint8_t)to_u8(o0);
-                    sp[1] = (uint8_t)to_u8(o1);
-                    sp[2] = (uint8_t)to_u8(o2);
-                }
-            } else {
-                // SKY_COLOR_U8 (135, 206, 235) packed
-                const uint32_t col = b >= 0 ? s_rgbp[b] : (135u | (206u << 8) | (235u << 16));
-                sp[0] = (uint8_t)col;
-                sp[1] = (uint8_t)(col >> 8);
-                sp[2] = (uint8_t)(col >> 16);
-            }
+    const float v = s_v[row0 + ly];
+    const float yraw = N::mad(v, c.uy, c.fy);
+    uint8_t* sp = stage + (ly * W + lx) * bpp;
+    for (int tx0 = 0; tx0 < W; tx0 += TW, sp += TW * bpp) {
+        const float u = s_u[tx0 + lx];
+        float x, y = yraw, z;
+        if (TRIG) {
+            x = N::mad(v, c.ux, N::mad(c.sy, c.cp, N::mul(u, c.rx)));
+            z = N::mad(v, c.uz, N::mad(c.cy, c.cp, N::mul(u, c.rz)));
+        } else {
+            x = N::mad(v, c.ux, N::mad(u, c.rx, c.fx));
+            z = N::mad(v, c.uz, N::mad(u, c.rz, c.fz));
         }
-        __syncwarp();
-        // copy the band (rows row0 .. row0+TH-1) out with 16-byte stores
-        const uint4* s4 = reinterpret_cast<const uint4*>(stage);
-        uint4* d4 = reinterpret_cast<uint4*>(oenv + (long long)row0 * W * bpp);
-        for (int k = lane; k < (band_bytes >> 4); k += 32) d4[k] = s4[k];
-        __syncwarp();
+        if (SHADED) {
+            const float len = N::sqrt(len2(x, y, z));
+            const float rl = N::rcp_of(len);
+            x = N::div_r(x, len, rl);
+            y = N::div_r(y, len, rl);
+            z = N::div_r(z, len, rl);
+        } else {
+            const float rs = N::rsqrt(len2(x, y, z));
+            x = N::mul(x, rs);
+            y = N::mul(y, rs);
+            z = N::mul(z, rs);
+        }
+        const float ix = (x != 0.0f) ? N::div(1.0f, x) : 1e30f;
+        const float iy = (y != 0.0f) ? N::div(1.0f, y) : 1e30f;
+        const float iz = (z != 0.0f) ? N::div(1.0f, z) : 1e30f;
+        const bool xp = x >= 0.0f, yp = y >= 0.0f, zp = z >= 0.0f;
+        float tmx = N::mul(xp ? d0.nxp : d0.nxm, ix);
+        float tmy = N::mul(yp ? d0.nyp : d0.nym, iy);
+        float tmz = N::mul(zp ? d0.nzp : d0.nzm, iz);
+        const int4 e = fe.start[(xp ? 1 : 0) | (yp ? 2 : 0) | (zp ? 4 : 0)];
+        const int b = SPLIT ? march_split_shared(fe.base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, fabsf(ix), fabsf(iy),
+                                                 fabsf(iz), fe.chk)
+                            : march_packed_shared(fe.base, e.x, e.y, e.z, e.w, tmx, tmy, tmz, fabsf(ix), fabsf(iy),
+                                                  fabsf(iz), fe.chk);
+        if (SHADED) {
+            // the axis of the last step, chosen again from the same distances
+            const bool bx = tmx < tmy && tmx < tmz;
+            const bool by = !bx && tmy < tmz;
+            const float t = bx ? tmx : (by ? tmy : tmz);
+            const bool hit = b >= 0 && !(t >= fe.vd);
+            const int code = bx ? 0 : (by ? (yp ? 3 : 2) : 1);
+            const float4 cs = s_cs[(b >= 0 ? b : 0) * 4 + code];
+            float fog = fminf(N::div_r(t, fe.vd, fe.rcp_vd), 1.0f);
+            fog = N::mul(fog, fog);
+            const float omf = N::sub(1.0f, fog);
+            const float c0 = (m & 1) ? N::mad(sky0, fog, N::mul(cs.x, omf)) : N::mad(cs.x, omf, N::mul(sky0, fog));
+            const float c1 = (m & 2) ? N::mad(sky1, fog, N::mul(cs.y, omf)) : N::mad(cs.y, omf, N::mul(sky1, fog));
+            const float c2 = (m & 4) ? N::mad(sky2, fog, N::mul(cs.z, omf)) : N::mad(cs.z, omf, N::mul(sky2, fog));
+            const float o0 = hit ? c0 : sky0, o1 = hit ? c1 : sky1, o2 = hit ? c2 : sky2;
+            if (F32) {
+                float* sf = reinterpret_cast<float*>(sp);
+                sf[0] = o0;
+                sf[1] = o1;
+                sf[2] = o2;
+            } else {
+                sp[0] = (uint8_t)to_u8(o0);
+                sp[1] = (uint8_t)to_u8(o1);
+                sp[2] = (uint8_t)to_u8(o2);
+            }
+        } else {
+            // SKY_COLOR_U8 (135, 206, 235) packed
+            const uint32_t col = b >= 0 ? s_rgbp[b] : (135u | (206u << 8) | (235u << 16));
+            sp[0] = (uint8_t)col;
+            sp[1] = (uint8_t)(col >> 8);
+            sp[2] = (uint8_t)(col >> 16);
+        }
     }
+    __syncwarp();
+    // copy the band (rows row0 .. row0+TH-1) out with 16-byte stores
+    const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+    uint4* d4 = reinterpret_cast<uint4*>(dst);
+    for (int k = lane; k < ((W * TH * bpp) >> 4); k += 32) d4[k] = s4[k];
+    __syncwarp();
+}
+
+// Start values of march_split_shared for an env whose eye is in voxel (vx,
+// vy, vz), one per sign combination k of the ray (as packed_start): {counts,
+// x, y and z address steps}; the start address is the eye voxel's.
+__device__ __forceinline__ int4 split_start(int k, int vx, int vy, int vz, int wx, int wy, int wz, int ytop,
+                                            int max_steps) {
+    const int sx = (k & 1) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 4) ? 1 : -1;
+    // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
+    const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
+              cz = (sz > 0) ? wz - 1 - vz : vz;
+    return make_int4(split_counts(cx, cy, cz, max_steps, wx, wy, wz), sx * wz, sy * wx * wz, sz);
+}
+
+// Whether an env takes the common-case loop, and which march: 0 no, 1
+// packed, 2 split.  `eye_air_inside`: the eye is strictly inside the box
+// (view distance > 0 for the shaded family) and its voxel holds air.
+template <int FAM>
+__device__ __forceinline__ int fast_kind(bool staged, bool eye_air_inside, bool dbg, bool vd_safe, int max_steps,
+                                         int wx, int wy, int wz, int W, int H, int TW, int bpp, bool vec_ok) {
+    if (!(FAM == MC_FAM_SHADED || FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS)) return 0;
+    if (!staged || !eye_air_inside || dbg || max_steps <= 0 || wx > 64 || wy > 64 || wz > 64) return 0;
+    if (W % TW || H % (32 / TW) || !vec_ok || ((W * (32 / TW) * bpp) & 15)) return 0;
+    const bool packed = (FAM == MC_FAM_SHADED ? vd_safe : true) && max_steps > wx + wy + wz && wx <= 31 &&
+                        wy <= 31 && wz <= 31 && wx * wy * wz < 8192;
+    return packed ? 1 : 2;
+}
+
+// The per-env start table (8 lanes write, the warp reads).
+__device__ __forceinline__ void build_fast_start(int4* sstart, int kind, const Dda0& d0, int wx, int wy, int wz,
+                                                 int ytop, int max_steps, int lane) {
+    if (lane < 8)
+        sstart[lane] = kind == 1 ? packed_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ytop)
+                                 : split_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ytop, max_steps);
+    __syncwarp();
 }
 
 // Per-env facts of a render (EnvRender::bits).
@@ -1968,17 +2024,9 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     FusedLayout L = fused_layout(W, H, wxyz, p.wx * p.wz, F32, STAGE, tile_w);
 
     // --- tables -------------------------------------------------------------
-    float4* s_cs = reinterpret_cast<float4*>(smem);                      // [13][4]
+    float4* s_cs = reinterpret_cast<float4*>(smem);                           // [13][4]
     uint32_t* s_rgbp = reinterpret_cast<uint32_t*>(smem + kShadeTableBytes);  // [13]
-    for (int k = threadIdx.x; k < 13 * 4; k += blockDim.x) {
-        // shade codes: 0 x face, 1 z face, 2 y face stepping down, 3 y face stepping up (shade_rgb)
-        const int blk = k >> 2, code = k & 3;
-        const float shade = code == 0 ? 0.8f : (code == 1 ? 0.9f : (code == 2 ? 0.6f : 1.0f));
-        s_cs[k] = make_float4(N::mul(c_rgb[blk][0], shade), N::mul(c_rgb[blk][1], shade),
-                              N::mul(c_rgb[blk][2], shade), 0.0f);
-    }
-    for (int k = threadIdx.x; k < 13; k += blockDim.x)
-        s_rgbp[k] = (uint32_t)c_rgb8[k][0] | ((uint32_t)c_rgb8[k][1] << 8) | ((uint32_t)c_rgb8[k][2] << 16);
+    build_fast_tables(s_cs, s_rgbp);
     float* s_u = reinterpret_cast<float*>(smem + kFastTableBytes);
     float* s_v = s_u + W;
     float (*s_rgb)[3] = reinterpret_cast<float (*)[3]>(s_v + H);
@@ -2211,12 +2259,26 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         }
         const int TW = L.tile_w, TH = L.tile_h;
         if constexpr (STAGE && (FAM == MC_FAM_SHADED || FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS)) {
-            // the common case: every ray takes the packed march over the staged
-            // world from the start-value table, no debug output, the image a
-            // whole number of tiles and bands that copy out in 16-byte pieces
-            if (start && !p.dbg_pixel && W % TW == 0 && H % TH == 0 && vec_ok && ((W * TH * bpp_of<F32>()) & 15) == 0) {
-                render_env_fast<FAM, F32>(c, d0, start, smem_u32(sworld), p.wx * p.wz, wxyz, p.vd, rcp_vd, W, H, TW,
-                                          lane, s_u, s_v, s_cs, s_rgbp, stage, oenv);
+            // the common case (fast_band): staged world, eye inside with air in
+            // its voxel, no debug output, whole tiles
+            const int fk = fast_kind<FAM>(true, sky_exit && skip_first, p.dbg_pixel != nullptr, vd_safe,
+                                          p.max_steps, p.wx, p.wy, p.wz, W, H, TW, 3 * (F32 ? 4 : 1), vec_ok);
+            if (fk) {
+                if (fk == 2 || !start) build_fast_start(sstart, fk, d0, p.wx, p.wy, p.wz, ytop, p.max_steps, lane);
+                const uint32_t wb = smem_u32(sworld);
+                FastEnv fe;
+                fe.start = sstart;
+                fe.base = fk == 1 ? wb : wb + (uint32_t)(d0.vy * wxz + d0.vx * p.wz + d0.vz);
+                fe.chk = staged_range(wb, wxz, wxyz);
+                fe.vd = p.vd;
+                fe.rcp_vd = rcp_vd;
+                for (int row0 = 0; row0 < H; row0 += TH) {
+                    uint8_t* dst = oenv + (long long)row0 * W * (3 * (F32 ? 4 : 1));
+                    if (fk == 1)
+                        fast_band<FAM, F32, false>(c, d0, fe, W, TW, row0, lane, s_u, s_v, s_cs, s_rgbp, stage, dst);
+                    else
+                        fast_band<FAM, F32, true>(c, d0, fe, W, TW, row0, lane, s_u, s_v, s_cs, s_rgbp, stage, dst);
+                }
                 continue;
             }
         }
@@ -2536,6 +2598,35 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
         if (lane == 0) v = atomicAdd(band_ctr, 1);
         return __shfl_sync(0xffffffffu, v, 0);
     };
+    if constexpr (std::is_same<V, VoxEither>::value &&
+                  (FAM == MC_FAM_SHADED || FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS)) {
+        // the common case (fast_band): staged world, eye inside with air in
+        // its voxel, no debug output, whole tiles
+        const int fk = fast_kind<FAM>(vox.smem, sky_exit && skip_first, dbg_pixel != nullptr, vd_safe, rp.max_steps,
+                                      rp.wx, rp.wy, rp.wz, W, H, TW, bpp, vec_ok);
+        if (fk) {
+            build_fast_start(cx.sstart, fk, d0, rp.wx, rp.wy, rp.wz, r.ytop, rp.max_steps, lane);
+            const uint32_t wb = staged_base(vox);
+            const int wxz = rp.wx * rp.wz;
+            FastEnv fe;
+            fe.start = cx.sstart;
+            fe.base = fk == 1 ? wb : wb + (uint32_t)(d0.vy * wxz + d0.vx * rp.wz + d0.vz);
+            fe.chk = staged_range(wb, wxz, wxz * rp.wy);
+            fe.vd = vd;
+            fe.rcp_vd = cx.rcp_vd;
+            for (int b = band_ctr ? claim() : 0; b < nbands; b = band_ctr ? claim() : b + 1) {
+                const int row0 = b * TH;
+                uint8_t* dst = oenv + (long long)row0 * W * bpp;
+                if (fk == 1)
+                    fast_band<FAM, F32, false>(r.c, d0, fe, W, TW, row0, lane, cx.s_u, cx.s_v, cx.s_cs, cx.s_rgbp,
+                                               cx.stage, dst);
+                else
+                    fast_band<FAM, F32, true>(r.c, d0, fe, W, TW, row0, lane, cx.s_u, cx.s_v, cx.s_cs, cx.s_rgbp,
+                                              cx.stage, dst);
+            }
+            return;
+        }
+    }
     for (int b = band_ctr ? claim() : 0; b < nbands; b = band_ctr ? claim() : b + 1) {
         const int row0 = b * TH;
         const int py = row0 + ly;
@@ -2682,6 +2773,10 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     // parameter blocks stay in the kernel's parameter space
     FusedCtx cx;
     load_colour_tables(smem, cx);
+    build_fast_tables(reinterpret_cast<float4*>(smem + MC_COLOUR_TABLE_BYTES),
+                      reinterpret_cast<uint32_t*>(smem + MC_COLOUR_TABLE_BYTES + kShadeTableBytes));
+    cx.s_cs = reinterpret_cast<const float4*>(smem + MC_COLOUR_TABLE_BYTES);
+    cx.s_rgbp = reinterpret_cast<const uint32_t*>(smem + MC_COLOUR_TABLE_BYTES + kShadeTableBytes);
     float* tables = reinterpret_cast<float*>(smem + rk.tables_off);
     for (int g = 0; g < G; ++g)
         build_uv_tables<FAM>(rk.groups[g], tables + rk.uv_off[g], tables + rk.uv_off[g] + rk.groups[g].W);
@@ -2689,7 +2784,8 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     int8_t* tworld = reinterpret_cast<int8_t*>(ts) + MC_TEAM_HEAD_BYTES;
     uint8_t* wbase = smem + rk.warps_off + warp * rk.warp_bytes;
     cx.mbar_a = smem_u32(wbase);
-    cx.stage = wbase + 16;
+    cx.sstart = reinterpret_cast<int4*>(wbase + 16);
+    cx.stage = wbase + 16 + 128;
     if (rk.stage_mask) mbar_init_warp(cx.mbar_a, lane);
     const bool claimer = (wt == 0 && lane == 0);
     const long long total_teams = (long long)gridDim.x * teams_per_cta;
@@ -2821,6 +2917,10 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
     const int G = rk.ngroups;
     FusedCtx cx;
     load_colour_tables(smem, cx);
+    build_fast_tables(reinterpret_cast<float4*>(smem + MC_COLOUR_TABLE_BYTES),
+                      reinterpret_cast<uint32_t*>(smem + MC_COLOUR_TABLE_BYTES + kShadeTableBytes));
+    cx.s_cs = reinterpret_cast<const float4*>(smem + MC_COLOUR_TABLE_BYTES);
+    cx.s_rgbp = reinterpret_cast<const uint32_t*>(smem + MC_COLOUR_TABLE_BYTES + kShadeTableBytes);
     float* tables = reinterpret_cast<float*>(smem + rk.tables_off);
     for (int g = 0; g < G; ++g)
         build_uv_tables<FAM>(rk.groups[g], tables + rk.uv_off[g], tables + rk.uv_off[g] + rk.groups[g].W);
@@ -2828,8 +2928,9 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
     int8_t* tworld = reinterpret_cast<int8_t*>(ts) + MC_TEAM_HEAD_BYTES;
     uint8_t* wbase = smem + rk.warps_off + warp * rk.warp_bytes;
     const uint32_t mbar0 = smem_u32(wbase);  // depth slot d's mbarrier at mbar0 + 8 d
-    EnvRender* stash = reinterpret_cast<EnvRender*>(wbase + 16);  // depth slot d's env at wbase + 16 + 96 d
-    cx.stage = wbase + 16 + 2 * MC_ENV_STASH_BYTES;
+    cx.sstart = reinterpret_cast<int4*>(wbase + 16);
+    EnvRender* stash = reinterpret_cast<EnvRender*>(wbase + 16 + 128);  // depth slot d's env at + 96 d
+    cx.stage = wbase + 16 + 128 + 2 * MC_ENV_STASH_BYTES;
     if (lane == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8) : "memory");

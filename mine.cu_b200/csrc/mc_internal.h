@@ -116,6 +116,9 @@ struct mc_fused_cfg {
 // Several env groups stepped by one launch of the team kernel (k_step_team).
 enum { MC_MAX_GROUPS = 16 };
 enum { MC_COLOUR_TABLE_BYTES = 224 };  // shared colour tables of the fused kernels (16-aligned)
+// the common-case render loop's tables (colour x shade: 13 x 4 float4; packed
+// flat colours: 13 uint32 padded to 64 bytes), after the colour tables
+enum { MC_FAST_TABLE_BYTES = 13 * 4 * 16 + 64 };
 enum { MC_TEAM_HEAD_BYTES = 128 };     // per-team shared words ahead of the team's world buffer
 enum { MC_ENV_STASH_BYTES = 96 };      // one env's render constants, kept in shared memory (depth 2)
 struct mc_ragged_kp {
@@ -148,8 +151,8 @@ struct mc_ragged_kp {
     int depth;                      // staging depth: 0 none, 1 one world buffer per stepper, 2 two (the
                                     // next unit's world is copied while the current one renders)
     int world_stride;               // bytes of one depth slot of a team's world region
-    int warp_bytes;                 // 16 (two mbarriers) [+ depth 2: two env stashes] + one band of
-                                    // observation bytes
+    int warp_bytes;                 // 16 (two mbarriers) + 128 (march start values) [+ depth 2: two env
+                                    // stashes] + one band of observation bytes
     int tail_bytes;                 // allocated after the warps: the march may read one world layer past the last world
 };
 

@@ -499,7 +499,7 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
         rk->ustart[v + 1] = rk->ustart[v] + (coop[g] ? B : (B + team_warps - 1) / team_warps);
     }
     rk->slot_bytes = slot;
-    rk->tables_off = MC_COLOUR_TABLE_BYTES;
+    rk->tables_off = MC_COLOUR_TABLE_BYTES + MC_FAST_TABLE_BYTES;
     rk->teams_off = rk->tables_off + align16i((long long)uv * 4);
     // the march reads up to one world layer (wx*wz bytes) on either side of a
     // staged world: worlds that follow one another are farther apart than
@@ -509,7 +509,8 @@ void team_layout(const mc_kp* const* kps, int G, const int* stage, const int* ti
     rk->world_stride = std::max(coop_world, team_warps * slot);
     rk->team_bytes = MC_TEAM_HEAD_BYTES + std::max(depth, 1) * rk->world_stride;
     rk->warps_off = rk->teams_off + (warps_per_cta / team_warps) * rk->team_bytes;
-    rk->warp_bytes = 16 + (depth == 2 ? 2 * MC_ENV_STASH_BYTES : 0) + band;
+    // per warp: two mbarriers, a table of march start values, [depth 2: two env stashes], one band
+    rk->warp_bytes = 16 + 128 + (depth == 2 ? 2 * MC_ENV_STASH_BYTES : 0) + band;
     const int after = warps_per_cta * rk->warp_bytes;
     rk->tail_bytes = after < pad ? pad - after : 0;
 }
