@@ -187,6 +187,10 @@ extern "C" const mc_backend* mc_backend_ieee();
 int mc_launch_reset_agents(const mc_kp* p, const uint8_t* mask, cudaStream_t s);
 int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s);
 int mc_launch_regen_if(const mc_kp* p, const uint8_t* flag, cudaStream_t s);
+// The conditional regeneration of up to MC_MAX_GROUPS groups in one launch
+// (groups that cannot end an episode are skipped; no launch when none can);
+// ctr is a counter word no other launch uses concurrently.
+int mc_launch_regen_groups(const mc_kp* const* kps, int G, int32_t* ctr, cudaStream_t s);
 
 // Record an error message for mc_last_error() and return `code`.
 int mc_set_error(int code, const char* msg);

@@ -297,6 +297,88 @@ int mc_launch_regen(const mc_kp* p, int conditional, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
+// The conditional regeneration of several env groups in one launch (a
+// ragged step, a server launch): each group whose any-done flag its step set
+// gets its worlds back (every world under the all-world rule, the worlds of
+// its done envs under the per-env rule), as mc_launch_regen would for that
+// group alone; one launch instead of one per group.
+namespace {
+struct RegenGroups {
+    int8_t* vox[MC_MAX_GROUPS];
+    const int8_t* tmpl[MC_MAX_GROUPS];
+    const uint8_t* do_reset[MC_MAX_GROUPS];
+    int32_t* flags[MC_MAX_GROUPS];
+    int B[MC_MAX_GROUPS];
+    int wxyz[MC_MAX_GROUPS];
+    int per_env[MC_MAX_GROUPS];
+    int G;
+    int32_t* ctr;  // finished CTAs of the launch (cleared by the last one)
+};
+
+__global__ void k_regen_groups(const __grid_constant__ RegenGroups rg) {
+    __shared__ int go[MC_MAX_GROUPS];
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    if (threadIdx.x < rg.G) {
+        go[threadIdx.x] = *(volatile int32_t*)&rg.flags[threadIdx.x][MC_FLAG_ANY_DONE] != 0;
+        if (go[threadIdx.x]) atomicOr(&any, 1);
+    }
+    __syncthreads();
+    // The flags were set before this launch and only its last CTA clears
+    // them: every CTA reads the same values, so when none is set none of them
+    // has anything to write, count or clear.
+    if (!any) return;
+    for (int g = 0; g < rg.G; ++g) {
+        if (!go[g]) continue;
+        const int wxyz = rg.wxyz[g];
+        const bool vec = (wxyz & 15) == 0 && ((((uintptr_t)rg.vox[g]) | ((uintptr_t)rg.tmpl[g])) & 15) == 0;
+        for (long long b = blockIdx.x; b < rg.B[g]; b += gridDim.x) {
+            if (rg.per_env[g] && !rg.do_reset[g][b]) continue;  // the same for every thread of the CTA
+            int8_t* d = rg.vox[g] + b * (long long)wxyz;
+            if (vec) {
+                uint4* d4 = reinterpret_cast<uint4*>(d);
+                const uint4* t4 = reinterpret_cast<const uint4*>(rg.tmpl[g]);
+                for (int k = threadIdx.x; k < (wxyz >> 4); k += blockDim.x) d4[k] = __ldg(t4 + k);
+            } else {
+                for (int k = threadIdx.x; k < wxyz; k += blockDim.x) d[k] = rg.tmpl[g][k];
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(reinterpret_cast<unsigned*>(rg.ctr), 1u);
+        if (prev == gridDim.x - 1) {
+            for (int g = 0; g < rg.G; ++g)
+                if (go[g]) rg.flags[g][MC_FLAG_ANY_DONE] = 0;
+            *rg.ctr = 0;
+            __threadfence();
+        }
+    }
+}
+}  // namespace
+
+int mc_launch_regen_groups(const mc_kp* const* kps, int G, int32_t* ctr, cudaStream_t s) {
+    RegenGroups rg{};
+    for (int g = 0; g < G; ++g) {
+        const mc_kp& k = *kps[g];
+        if (k.B == 0 || !dones_possible(k)) continue;
+        const int i = rg.G++;
+        rg.vox[i] = k.voxels;
+        rg.tmpl[i] = k.world_template;
+        rg.do_reset[i] = k.do_reset;
+        rg.flags[i] = k.flags;
+        rg.B[i] = k.B;
+        rg.wxyz[i] = k.wx * k.wy * k.wz;
+        rg.per_env[i] = k.regen_per_env;
+    }
+    if (rg.G == 0) return 0;
+    rg.ctr = ctr;
+    k_regen_groups<<<1184, 256, 0, s>>>(rg);  // 148 SMs x 8
+    return (int)cudaGetLastError();
+}
+
 namespace {
 __global__ void k_flag_from_byte(int32_t* flags, const uint8_t* flag) {
     flags[MC_FLAG_ANY_DONE] = *flag ? 1 : 0;
@@ -1327,12 +1409,10 @@ static int ragged_do_step(mc_ragged* r, const int8_t* buttons, const float* look
                                      r->num_sms, s),
                     "step_team");
     if (rc) return rc;
-    for (auto* e : r->envs)
-        if (e->cfg.batch_size > 0 && dones_possible(e->kp)) {
-            rc = backend_rc(mc_launch_regen(&e->kp, 1, s), "regen");
-            if (rc) return rc;
-        }
-    return MC_OK;
+    std::vector<const mc_kp*> kps;
+    for (auto* e : r->envs) kps.push_back(&e->kp);
+    return backend_rc(mc_launch_regen_groups(kps.data(), (int)kps.size(), r->flags + MC_FLAG_REGEN_CTR, s),
+                      "regen");
 }
 
 extern "C" int mc_ragged_step(mc_ragged* r, const int8_t* buttons, const float* look, void* stream) {

@@ -374,11 +374,8 @@ int run_round(mc_server* s, Slot& sl, const std::vector<Req*>& reqs, const std::
             const mc_kp& k0 = *kps[0];
             rc = s->be->step_team(&rk, k0.family, k0.obs_f32, 8, cps, s->num_sms, st);
             if (rc) return mc_cuda_fail((cudaError_t)rc, "server: step launch");
-            for (int g = 0; g < G && rc == MC_OK; ++g)
-                if (dones_possible(*kps[g])) {
-                    rc = mc_launch_regen(kps[g], 1, st);
-                    if (rc) return mc_cuda_fail((cudaError_t)rc, "server: regeneration");
-                }
+            rc = mc_launch_regen_groups(kps.data(), G, s->flags + MC_FLAG_REGEN_CTR, st);
+            if (rc) return mc_cuda_fail((cudaError_t)rc, "server: regeneration");
         } else {
             Req* r = reqs[steps[0]];
             rc = mc_env_step_discrete(r->job->env, d_act, MC_FORM_PLAIN, st);
