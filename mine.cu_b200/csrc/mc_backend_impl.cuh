@@ -2011,8 +2011,12 @@ __device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long 
 #ifndef MC_FUSED_MIN_BLOCKS
 #define MC_FUSED_MIN_BLOCKS 4
 #endif
-template <int FAM, bool F32, bool STAGE>
+// DEPTH: 0 worlds read from global memory, 1 staged, 2 staged with the next
+// env claimed ahead and its world prefetched into L2.
+template <int FAM, bool F32, int DEPTH>
 __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const __grid_constant__ mc_kp p, int tile_w) {
+    constexpr bool STAGE = DEPTH > 0;
+    constexpr bool prefetch = DEPTH == 2;
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -2075,7 +2079,31 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     const long long total_warps = (long long)gridDim.x * nwarps;
     const long long first = p.sched_dynamic ? next_env(p, 0, total_warps, lane) : (long long)blockIdx.x * nwarps + warp;
     long long e = first;
-    for (; e < p.B; e = next_env(p, e, total_warps, lane)) {
+    // staging depth 2 (prefetch): the warp claims its next env one ahead and,
+    // while it steps and renders this one, prefetches that env's world (and
+    // the state the step reads) into L2, so the next bulk copy reads L2
+    long long ahead = (prefetch && e < p.B) ? next_env(p, e, total_warps, lane) : p.B;
+    auto advance = [&]() -> long long {
+        if (!prefetch) return next_env(p, e, total_warps, lane);
+        const long long r = ahead;
+        ahead = r < p.B ? next_env(p, r, total_warps, lane) : r;
+        return r;
+    };
+    for (; e < p.B; e = advance()) {
+        if (prefetch && ahead < p.B) {
+            if (lane == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p.voxels + ahead * (long long)wxyz),
+                             "r"(wxyz)
+                             : "memory");
+            const void* st = lane == 1 ? (const void*)(p.positions + ahead * 3)
+                           : lane == 2 ? (const void*)(p.velocities + ahead * 3)
+                           : lane == 3 ? (const void*)(p.yaws + ahead)
+                           : lane == 4 ? (const void*)(p.pitches + ahead)
+                           : lane == 5 ? (const void*)(p.on_ground + ahead)
+                           : lane == 6 && p.actions ? (const void*)(p.actions + ahead)
+                                                    : nullptr;
+            if (st) asm volatile("prefetch.global.L2 [%0];" ::"l"(st));
+        }
         // ---- agent step (every lane computes the same values) --------------
         int8_t btn[8];
         float l0, l1;
@@ -3149,9 +3177,9 @@ static size_t fused_smem(const mc_kp* p, const mc_fused_cfg* cfg) {
     return (size_t)L.head_bytes + (size_t)cfg->warps_per_cta * L.warp_bytes + (size_t)L.pad_bytes;
 }
 
-template <int FAM, bool F32, bool STAGE>
+template <int FAM, bool F32, int DEPTH>
 static int launch_fused_t(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
-    auto kern = k_step_fused<FAM, F32, STAGE>;
+    auto kern = k_step_fused<FAM, F32, DEPTH>;
     size_t smem = fused_smem(p, cfg);
     static size_t attr_set = 0;  // per instantiation
     if (smem > 48 * 1024 && smem > attr_set) {
@@ -3170,8 +3198,8 @@ static int launch_fused_t(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, 
 
 template <int FAM, bool F32>
 static int launch_fused_f(const mc_kp* p, const mc_fused_cfg* cfg, int num_sms, cudaStream_t s) {
-    return cfg->stage ? launch_fused_t<FAM, F32, true>(p, cfg, num_sms, s)
-                      : launch_fused_t<FAM, F32, false>(p, cfg, num_sms, s);
+    if (cfg->stage == 2) return launch_fused_t<FAM, F32, 2>(p, cfg, num_sms, s);
+    return cfg->stage ? launch_fused_t<FAM, F32, 1>(p, cfg, num_sms, s) : launch_fused_t<FAM, F32, 0>(p, cfg, num_sms, s);
 }
 
 template <int FAM, bool F32>

@@ -639,8 +639,8 @@ static int validate_fused_kp(const mc_env_config* cfg, const mc_kp* kp, const mc
                              f->ctas_per_sm);
     }
     if (f->team_warps != 1) return fail(MC_ERR_INVALID, "team_warps must be 1 without coop");
-    if (f->stage != 0 && f->stage != 1)
-        return fail(MC_ERR_INVALID, "one warp per env stages at depth 0 or 1 (depth 2 needs a team launch)");
+    if (f->stage < 0 || f->stage > 2)
+        return fail(MC_ERR_INVALID, "stage (staging depth) must be 0, 1 or 2");
     if (f->warps_per_cta != 4 && f->warps_per_cta != 8)
         return fail(MC_ERR_INVALID, "warps_per_cta must be 4 or 8");
     if (f->tile_w != 4 && f->tile_w != 8 && f->tile_w != 16 && f->tile_w != 32)

@@ -9,9 +9,11 @@ own envs:
                     (32 / tile_w) rays (one ray per lane: rays per warp
                     iteration = 32, in rows of tile_w; 4, 8, 16 or 32);
 * ``stage``         staging depth of the worlds in shared memory: 0 none, 1
-                    one world buffer per stepping warp, 2 two (team launches:
-                    the next unit's world is copied while the current one
-                    renders);
+                    one world buffer per stepping warp, 2 one more env in
+                    flight (team launches: the next unit's world is copied
+                    into a second buffer while the current one renders; one
+                    warp per env: the next env is claimed ahead and its world
+                    prefetched into L2);
 * ``team_warps``    warps per team (1, 2, 4, 8);
 * ``coop``          1: a team renders each env together (envs per CTA =
                     teams per CTA); 0: each warp its own env (envs per CTA =
@@ -106,7 +108,7 @@ def _actions(n_envs: int, steps: int, seed: int, device) -> torch.Tensor:
 # ---------------------------------------------------------------------------
 def env_candidates() -> List[Tuple[int, int, int, int, int, int]]:
     """(stage, warps_per_cta, ctas_per_sm, tile_w, team_warps, coop) tried by tune_env."""
-    per_warp = [(st, wpc, cps, tw, 1, 0) for st in (0, 1) for wpc in (4, 8) for cps in (2, 4, 8)
+    per_warp = [(st, wpc, cps, tw, 1, 0) for st in (0, 1, 2) for wpc in (4, 8) for cps in (2, 4, 8)
                 for tw in TILE_WIDTHS]
     teams = [(st, 8, cps, tw, team, 1) for st in (0, 1, 2) for cps in (2, 3, 4) for tw in TILE_WIDTHS
              for team in (2, 4, 8)]

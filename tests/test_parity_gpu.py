@@ -64,7 +64,7 @@ def test_c1_uint8_ieee_bit_exact(cuda, form):
     run_vs_oracle(cuda, 100, 0, form)
 
 
-@pytest.mark.parametrize("stage", [0, 1])
+@pytest.mark.parametrize("stage", [0, 1, 2])
 def test_fused_staged_and_direct_bit_exact(cuda, stage):
     run_vs_oracle(cuda, 40, 5, FUSED, stage=stage, B=40)
 
@@ -123,8 +123,8 @@ EARLY_EXIT_CASES = {
 
 @pytest.mark.parametrize("case", sorted(EARLY_EXIT_CASES))
 @pytest.mark.parametrize("mode", ["uint8", "uint8_minimal"])
-@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1), (2, 8, 2, 8, 4, 1)],
-                         ids=["per_warp", "team", "team_depth2"])
+@pytest.mark.parametrize("cfg", [(1, 8, 4, 4, 1, 0), (1, 8, 3, 8, 4, 1), (2, 8, 2, 8, 4, 1), (2, 8, 4, 4, 1, 0)],
+                         ids=["per_warp", "team", "team_depth2", "per_warp_depth2"])
 def test_early_exit_march_vs_oracle(cuda, case, mode, cfg):
     """The fused kernels without debug outputs, where the march over a
     staged world ends rays early (left the box, above the highest solid

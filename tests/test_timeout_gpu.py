@@ -22,6 +22,7 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = {
     "per_warp": (1, 8, 4, 4, 1, 0),
+    "per_warp_depth2": (2, 8, 4, 4, 1, 0),
     "team_coop": (1, 8, 3, 8, 4, 1),
     "team_per_warp": (1, 8, 3, 4, 2, 0),
     "team_coop_depth2": (2, 8, 2, 8, 4, 1),
