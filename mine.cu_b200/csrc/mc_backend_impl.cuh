@@ -722,16 +722,60 @@ __device__ __forceinline__ int march_packed_shared(uint32_t world, int packed, i
 #endif
 }
 
+// Where a ray going up from the eye's voxel (vx, vy, vz) can still meet a
+// solid voxel, per quadrant q of the eye's column (bit 0: the x >= vx side,
+// bit 1: the z >= vz side; each side includes the eye's own row): such a
+// ray only visits voxels with y >= vy on its quadrant's sides, so once it
+// is past the extreme x, the extreme z or the highest layer of the solid
+// voxels there it meets none again and ends as sky, as the full march
+// would.  One byte per quadrant: x = the largest x (x >= vx side) or the
+// smallest (x <= vx side), z likewise, y = the highest layer + 1 (0: none).
+struct UpBounds {
+    uint32_t x, z, y;
+};
+
+// Bounds that cut nothing but the layers above ytop (every quadrant's x and
+// z extremes at the box's faces).
+__device__ __forceinline__ UpBounds up_none(int ytop) {
+    return UpBounds{0xFF00FF00u, 0xFFFF0000u, (uint32_t)(min(max(ytop, -1), 254) + 1) * 0x01010101u};
+}
+
+// The highest solid layer at or above vy (-1: none), from the bounds: every
+// solid voxel at or above the eye's layer lies in some quadrant.
+__device__ __forceinline__ int up_top(const UpBounds& b) {
+    return (int)max(max(b.y & 255u, (b.y >> 8) & 255u), max((b.y >> 16) & 255u, b.y >> 24)) - 1;
+}
+
+// In-box step counts of a march from the eye's voxel for ray sign
+// combination k (bit 0: x >= 0, bit 1: y >= 0, bit 2: z >= 0): the steps
+// left to each face of the box, cut for a ray going up by its quadrant's
+// bounds; a count of -1 ends the ray (as sky) at its first step.
+__device__ __forceinline__ void start_counts(int k, int vx, int vy, int vz, int wx, int wy, int wz,
+                                             const UpBounds& ub, int& cx, int& cy, int& cz) {
+    const bool px = k & 1, py = k & 2, pz = k & 4;
+    cx = px ? wx - 1 - vx : vx;
+    cy = py ? wy - 1 - vy : vy;
+    cz = pz ? wz - 1 - vz : vz;
+    if (py) {
+        const int sh = 8 * ((px ? 1 : 0) | (pz ? 2 : 0));
+        const int xe = (ub.x >> sh) & 255, ze = (ub.z >> sh) & 255, yt = (int)((ub.y >> sh) & 255) - 1;
+        cx = max(min(cx, px ? xe - vx : vx - xe), -1);
+        cz = max(min(cz, pz ? ze - vz : vz - ze), -1);
+        cy = max(min(cy, yt - vy), -1);
+    }
+}
+
 // Start values of march_packed_shared for an env whose eye is in voxel
 // (vx, vy, vz), one per sign combination k of the ray (bit 0: x >= 0, bit 1:
 // y >= 0, bit 2: z >= 0): {packed index and counts, x, y and z increments}.
-__device__ __forceinline__ int4 packed_start(int k, int vx, int vy, int vz, int wx, int wy, int wz, int ytop) {
+// Counts from start_counts (at least -1, at most 31).
+__device__ __forceinline__ int4 packed_start(int k, int vx, int vy, int vz, int wx, int wy, int wz,
+                                             const UpBounds& ub) {
     const int sx = (k & 1) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 4) ? 1 : -1;
     const int wxz = wx * wz, idx = vy * wxz + vx * wz + vz;
-    // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
-    const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
-              cz = (sz > 0) ? wz - 1 - vz : vz;
-    return make_int4((idx << 18) | ((31 - cx) << 12) | ((31 - max(cy, -32)) << 6) | (31 - cz),
+    int cx, cy, cz;
+    start_counts(k, vx, vy, vz, wx, wy, wz, ub, cx, cy, cz);
+    return make_int4((idx << 18) | ((31 - cx) << 12) | ((31 - cy) << 6) | (31 - cz),
                      ((sx * wz) << 18) + (1 << 12), ((sy * wxz) << 18) + (1 << 6), (sz << 18) + 1);
 }
 
@@ -1843,6 +1887,92 @@ __device__ __forceinline__ int staged_top_layer(const int8_t* world, int wx, int
     return __reduce_max_sync(0xffffffffu, top);
 }
 
+// Solid voxels (byte >= 0) of 16 consecutive bytes as a 16-bit mask: per
+// 32-bit word the four sign bits (7, 15, 23, 31) of ~w, multiplied by
+// 1 + 2^7 + 2^14 + 2^21, land on bits 28..31 with no carries.
+__device__ __forceinline__ uint32_t solid_mask16(uint4 q) {
+    auto four = [](uint32_t w) { return ((~w & 0x80808080u) * 0x00204081u) >> 28; };
+    return four(q.x) | (four(q.y) << 4) | (four(q.z) << 8) | (four(q.w) << 12);
+}
+
+// Whether staged_up_bounds can scan a world of this shape: whole 16-byte
+// chunks per row of z, at most 64 voxels a side.
+__host__ __device__ __forceinline__ bool up_scan_shape(int wx, int wy, int wz) {
+    return (wz & 15) == 0 && wz <= 64 && wx <= 64 && wy <= 64;
+}
+
+// One warp scans the rows (y >= vy, x) of a staged world (up_scan_shape;
+// the eye's voxel inside the box) for the bounds of every quadrant.  Each
+// lane keeps one x (two in worlds wider than 32): G = 32 / wx groups of wx
+// lanes sweep every G-th layer, so per row a lane only ORs the row's solid
+// z mask into its column's union and notes the highest layers with a solid
+// voxel at z >= vz and at z <= vz; the column's x side and the z extremes
+// are settled once, after the sweep.
+template <typename M>
+__device__ __forceinline__ UpBounds staged_up_bounds_t(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
+                                                       int vz, int lane) {
+    constexpr int kBits = 8 * sizeof(M);
+    const int cpr = wz >> 4;                              // 16-byte chunks per row
+    const M zpm = ~M(0) << vz;                            // z >= vz
+    const M zmm = (vz + 1 < kBits) ? ((M(1) << (vz + 1)) - 1) : ~M(0);  // z <= vz
+    const int G = wx <= 32 ? 32 / wx : 1, g = wx <= 32 ? lane / wx : 0;
+    int xa0 = 255, xa1 = 0, xa2 = 255, xa3 = 0;  // x extremes of q0 (x-, z-), q1 (x+, z-), q2 (x-, z+), q3 (x+, z+)
+    int ya0 = 0, ya1 = 0, ya2 = 0, ya3 = 0;      // highest layer + 1
+    M mp = 0, mm = 0;                            // solid z masks of the x >= vx / x <= vx columns
+    for (int x = wx <= 32 ? lane - g * wx : lane; g < G && x < wx; x += 32) {
+        M mu = 0;
+        int yp = 0, ym = 0;  // highest layer + 1 with a solid voxel at z >= vz / z <= vz
+        for (int y = vy + g; y < wy; y += G) {
+            const int r = y * wx + x;
+            const uint4* row = reinterpret_cast<const uint4*>(world + r * wz);
+            M m = 0;
+            for (int k = 0; k < cpr; ++k) {
+                const uint4 q = in_bounds((long long)r * cpr + k, (long long)wx * wy * cpr, MC_SITE_SCAN)
+                                    ? row[k] : make_uint4(~0u, ~0u, ~0u, ~0u);
+                m |= M(solid_mask16(q)) << (16 * k);
+            }
+            mu |= m;
+            yp = (m & zpm) ? y + 1 : yp;
+            ym = (m & zmm) ? y + 1 : ym;
+        }
+        if (x >= vx) {
+            mp |= mu;
+            if (yp) { xa3 = max(xa3, x); ya3 = max(ya3, yp); }
+            if (ym) { xa1 = max(xa1, x); ya1 = max(ya1, ym); }
+        }
+        if (x <= vx) {
+            mm |= mu;
+            if (yp) { xa2 = min(xa2, x); ya2 = max(ya2, yp); }
+            if (ym) { xa0 = min(xa0, x); ya0 = max(ya0, ym); }
+        }
+    }
+    constexpr unsigned F = 0xffffffffu;
+    auto or_all = [](M v) -> M {
+        if (sizeof(M) == 8)
+            return M(__reduce_or_sync(F, (unsigned)v)) | (M(__reduce_or_sync(F, (unsigned)(v >> 16 >> 16))) << 16 << 16);
+        return M(__reduce_or_sync(F, (unsigned)v));
+    };
+    auto hi = [](M v) { return kBits - 1 - (sizeof(M) == 8 ? __clzll((long long)v) : __clz((int)v)); };
+    auto lo = [](M v) { return (sizeof(M) == 8 ? __ffsll((long long)v) : __ffs((int)v)) - 1; };
+    mp = or_all(mp);
+    mm = or_all(mm);
+    // z extremes: over a side's solid voxels the largest z is the z >= vz quadrant's extreme whenever that
+    // quadrant holds any (else its y byte is 0 and the value is not used), the smallest z likewise
+    UpBounds b;
+    b.x = (unsigned)__reduce_min_sync(F, xa0) | ((unsigned)__reduce_max_sync(F, xa1) << 8) |
+          ((unsigned)__reduce_min_sync(F, xa2) << 16) | ((unsigned)__reduce_max_sync(F, xa3) << 24);
+    b.z = ((unsigned)lo(mm) & 255u) | (((unsigned)lo(mp) & 255u) << 8) | (((unsigned)hi(mm) & 255u) << 16) |
+          (((unsigned)hi(mp) & 255u) << 24);
+    b.y = (unsigned)__reduce_max_sync(F, ya0) | ((unsigned)__reduce_max_sync(F, ya1) << 8) |
+          ((unsigned)__reduce_max_sync(F, ya2) << 16) | ((unsigned)__reduce_max_sync(F, ya3) << 24);
+    return b;
+}
+__device__ __forceinline__ UpBounds staged_up_bounds(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
+                                                     int vz, int lane) {
+    return wz > 32 ? staged_up_bounds_t<unsigned long long>(world, wx, wy, wz, vx, vy, vz, lane)
+                   : staged_up_bounds_t<uint32_t>(world, wx, wy, wz, vx, vy, vz, lane);
+}
+
 // ---------------------------------------------------------------------------
 // Fused step, one warp per env (one env group per launch)
 // ---------------------------------------------------------------------------
@@ -1964,12 +2094,11 @@ __device__ __forceinline__ void fast_band(const Cam& c, const Dda0& d0, const Fa
 // Start values of march_split_shared for an env whose eye is in voxel (vx,
 // vy, vz), one per sign combination k of the ray (as packed_start): {counts,
 // x, y and z address steps}; the start address is the eye voxel's.
-__device__ __forceinline__ int4 split_start(int k, int vx, int vy, int vz, int wx, int wy, int wz, int ytop,
-                                            int max_steps) {
+__device__ __forceinline__ int4 split_start(int k, int vx, int vy, int vz, int wx, int wy, int wz,
+                                            const UpBounds& ub, int max_steps) {
     const int sx = (k & 1) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 4) ? 1 : -1;
-    // a ray going up stops above ytop (no solid voxel lies higher): it ends as sky
-    const int cx = (sx > 0) ? wx - 1 - vx : vx, cy = (sy > 0) ? min(wy - 1, ytop) - vy : vy,
-              cz = (sz > 0) ? wz - 1 - vz : vz;
+    int cx, cy, cz;
+    start_counts(k, vx, vy, vz, wx, wy, wz, ub, cx, cy, cz);
     return make_int4(split_counts(cx, cy, cz, max_steps, wx, wy, wz), sx * wz, sy * wx * wz, sz);
 }
 
@@ -1989,10 +2118,10 @@ __device__ __forceinline__ int fast_kind(bool staged, bool eye_air_inside, bool 
 
 // The per-env start table (8 lanes write, the warp reads).
 __device__ __forceinline__ void build_fast_start(int4* sstart, int kind, const Dda0& d0, int wx, int wy, int wz,
-                                                 int ytop, int max_steps, int lane) {
+                                                 const UpBounds& ub, int max_steps, int lane) {
     if (lane < 8)
-        sstart[lane] = kind == 1 ? packed_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ytop)
-                                 : split_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ytop, max_steps);
+        sstart[lane] = kind == 1 ? packed_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ub)
+                                 : split_start(lane, d0.vx, d0.vy, d0.vz, wx, wy, wz, ub, max_steps);
     __syncwarp();
 }
 
@@ -2233,6 +2362,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         // ---- stage the world into shared memory ----------------------------
         const int8_t* wsrc = gw;
         int ytop = p.wy - 1;  // highest layer with a solid voxel (all layers unless measured)
+        UpBounds ub = up_none(ytop);
         if (STAGE) {
 #if MC_CHECK_BOUNDS
             {
@@ -2266,7 +2396,13 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
             if (lane == 0 && mod_idx >= 0 && in_bounds(mod_idx, wxyz, MC_SITE_PATCH)) sworld[mod_idx] = mod_val;
             __syncwarp();
             wsrc = sworld;
-            ytop = staged_top_layer(sworld, p.wx, p.wy, p.wz, lane);
+            if (eye_inb && up_scan_shape(p.wx, p.wy, p.wz)) {
+                ub = staged_up_bounds(sworld, p.wx, p.wy, p.wz, ex, ey, ez, lane);
+                ytop = up_top(ub);  // the same cut for rays going up from the eye
+            } else {
+                ytop = staged_top_layer(sworld, p.wx, p.wy, p.wz, lane);
+                ub = up_none(ytop);
+            }
         }
         // ---- march every pixel ---------------------------------------------
         const Dda0 d0 = dda0(c);
@@ -2281,7 +2417,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         const bool flat_fam = FAM == MC_FAM_MINIMAL || FAM == MC_FAM_PREBASIS;
         if (STAGE && (FAM == MC_FAM_SHADED ? vd_safe : (flat_fam && sky_exit)) &&
             p.max_steps > p.wx + p.wy + p.wz && p.wx <= 31 && p.wy <= 31 && p.wz <= 31 && wxyz < 8192) {
-            if (lane < 8) sstart[lane] = packed_start(lane, d0.vx, d0.vy, d0.vz, p.wx, p.wy, p.wz, ytop);
+            if (lane < 8) sstart[lane] = packed_start(lane, d0.vx, d0.vy, d0.vz, p.wx, p.wy, p.wz, ub);
             __syncwarp();
             start = sstart;
         }
@@ -2292,7 +2428,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
             const int fk = fast_kind<FAM>(true, sky_exit && skip_first, p.dbg_pixel != nullptr, vd_safe,
                                           p.max_steps, p.wx, p.wy, p.wz, W, H, TW, 3 * (F32 ? 4 : 1), vec_ok);
             if (fk) {
-                if (fk == 2 || !start) build_fast_start(sstart, fk, d0, p.wx, p.wy, p.wz, ytop, p.max_steps, lane);
+                if (fk == 2 || !start) build_fast_start(sstart, fk, d0, p.wx, p.wy, p.wz, ub, p.max_steps, lane);
                 const uint32_t wb = smem_u32(sworld);
                 FastEnv fe;
                 fe.start = sstart;
@@ -2433,7 +2569,22 @@ struct EnvRender {
     int mod_idx;   // voxel index the interaction wrote, -1 if none
     int mod_val;
     int ytop;      // no solid voxel above this layer (wy - 1 unless measured)
+    UpBounds ub;   // bounds of the rays going up (up_none(ytop) unless measured)
 };
+
+// Measure a staged world for the rays going up: per quadrant of the eye's
+// column when the eye's voxel lies in the box, else the top layer only.
+__device__ __forceinline__ void measure_staged(EnvRender& r, const int8_t* world, int wx, int wy, int wz, int lane) {
+    const int ex = (int)floorf(r.c.eye_x), ey = (int)floorf(r.c.eye_y), ez = (int)floorf(r.c.eye_z);
+    if ((unsigned)ex < (unsigned)wx && (unsigned)ey < (unsigned)wy && (unsigned)ez < (unsigned)wz &&
+        up_scan_shape(wx, wy, wz)) {
+        r.ub = staged_up_bounds(world, wx, wy, wz, ex, ey, ez, lane);
+        r.ytop = up_top(r.ub);
+    } else {
+        r.ytop = staged_top_layer(world, wx, wy, wz, lane);
+        r.ub = up_none(r.ytop);
+    }
+}
 
 
 struct TeamShared {
@@ -2523,6 +2674,7 @@ __device__ __forceinline__ EnvRender agent_step(const mc_kp& p, const ActionSrc&
     r.mod_idx = mod_idx;
     r.mod_val = mod_val;
     r.ytop = p.wy - 1;
+    r.ub = up_none(r.ytop);
     return r;
 }
 
@@ -2633,7 +2785,7 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
         const int fk = fast_kind<FAM>(vox.smem, sky_exit && skip_first, dbg_pixel != nullptr, vd_safe, rp.max_steps,
                                       rp.wx, rp.wy, rp.wz, W, H, TW, bpp, vec_ok);
         if (fk) {
-            build_fast_start(cx.sstart, fk, d0, rp.wx, rp.wy, rp.wz, r.ytop, rp.max_steps, lane);
+            build_fast_start(cx.sstart, fk, d0, rp.wx, rp.wy, rp.wz, r.ub, rp.max_steps, lane);
             const uint32_t wb = staged_base(vox);
             const int wxz = rp.wx * rp.wz;
             FastEnv fe;
@@ -2742,6 +2894,7 @@ __device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long 
         r.mod_idx = -1;
         r.mod_val = 0;
         r.ytop = p.wy - 1;
+        r.ub = up_none(r.ytop);
         render_env<FAM, F32, VoxGlobal, false>(p, e, r, cx, VoxGlobal{p.voxels + e * wxyz}, tile_w, lane, nullptr);
         e = next_env(p, e, total_warps, lane);
     }
@@ -2880,7 +3033,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                     if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
                         world[r.mod_idx] = (int8_t)r.mod_val;
                     __syncwarp();
-                    r.ytop = staged_top_layer(world, p.wx, p.wy, p.wz, lane);
+                    measure_staged(r, world, p.wx, p.wy, p.wz, lane);
                 } else {
                     if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
                     warp_no_stage = true;  // the copy may still land: render from global memory from now on
@@ -3060,7 +3213,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
                 if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
                     world[r.mod_idx] = (int8_t)r.mod_val;
                 __syncwarp();
-                r.ytop = staged_top_layer(world, p.wx, p.wy, p.wz, lane);
+                measure_staged(r, world, p.wx, p.wy, p.wz, lane);
             } else {
                 if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
                 warp_no_stage = true;  // the copy may still land: render from global memory from now on

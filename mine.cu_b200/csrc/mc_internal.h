@@ -42,6 +42,7 @@ enum {
     MC_SITE_PATCH = 11,        // the interaction's voxel patched into the staged world
     MC_SITE_TABLE = 12,        // u/v tables, colour tables
     MC_SITE_STAGE = 13,        // a bulk copy's destination vs the CTA's dynamic shared memory
+    MC_SITE_SCAN = 14,         // a staged world's rows read by the up-bounds scan
 };
 
 // Polls of an mbarrier before a bulk-copy wait gives up (each poll is one
