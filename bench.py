@@ -837,6 +837,82 @@ def reference_legs(args, dev, W):
     return legs
 
 
+REF_PKG = os.path.join(ROOT, "baseline", "_ref")
+STATE_KEYS = ("voxels", "positions", "velocities", "yaws", "pitches", "on_ground", "step_count", "do_reset",
+              "cameras", "rewards", "obs_buffer")
+
+
+def run_stock_leg(args):
+    """--stock-leg (run by the reference arm in a child process): the
+    headline window through the reference package itself, built by its own
+    setup.py into baseline/_ref: minecu.MineEnv(...).step(buttons, look)
+    with persistent action buffers (its graphs keep the action pointers,
+    src/kernels.cu:2526-2542).  After the window, every state tensor is
+    compared bit for bit with the restated driver (oracle/ref_driver.py)
+    stepped with the same actions: that is the check that the reference
+    arm's driver runs the reference's own step."""
+    import torch
+    sys.path[:] = [q for q in sys.path if os.path.abspath(q) != os.path.join(ROOT, "mine.cu_b200")]
+    sys.path.insert(0, REF_PKG)
+    sys.path.insert(1, os.path.join(ROOT, "oracle"))
+    import minecu as stock
+    if not os.path.abspath(stock.__file__).startswith(REF_PKG):
+        raise RuntimeError(f"expected the reference package from {REF_PKG}, got {stock.__file__}")
+    import oracle as O
+    import ref_driver
+    W = workload(args)
+    B, K, Wm = W["batch_size"], args.steps, args.warmup
+    dev = torch.device("cuda", 0)
+    btns = torch.empty((K + Wm, B, 8), dtype=torch.int8)
+    looks = torch.empty((K + Wm, B, 2), dtype=torch.float32)
+    for s in range(K + Wm):
+        b, l = O.discrete_to_buttons(O.philox_actions(B, s, W["seed"], break_half=W["break_half"]), W["look_delta"])
+        btns[s] = torch.from_numpy(b)
+        looks[s] = torch.from_numpy(l)
+    d_btn, d_look = btns.to(dev), looks.to(dev)
+    kw = dict(batch_size=B, world_size=W["world"], render_width=W["res"], render_height=W["res"], device=str(dev),
+              max_steps=W["max_steps"], obs_dtype=W["obs_dtype"], target_block=3)
+    env = stock.MineEnv(**kw)
+    pb = torch.zeros((B, 8), dtype=torch.int8, device=dev)
+    pl = torch.zeros((B, 2), dtype=torch.float32, device=dev)
+
+    def step(s):
+        pb.copy_(d_btn[s])
+        pl.copy_(d_look[s])
+        env.step(pb, pl)
+    env.reset()
+    for s in range(Wm):
+        step(s)
+    t = _event_time(lambda: [step(Wm + s) for s in range(K)])
+    ref = ref_driver.RefEnv(**kw)
+    ref.reset()
+    for s in range(Wm + K):
+        ref.step(d_btn[s], d_look[s])
+    torch.cuda.synchronize()
+
+    def bits(x):
+        return x.view(torch.int32) if x.dtype == torch.float32 else x
+    differ = [k for k in STATE_KEYS if not torch.equal(bits(getattr(env, k)), bits(getattr(ref, k)))]
+    print("STOCK " + json.dumps({
+        "path": "baseline/_ref: the reference package built by its own setup.py (pip install --target, "
+                "TORCH_CUDA_ARCH_LIST=10.0a), minecu.MineEnv.step(buttons, look), default stream",
+        "value": B * K / t, "unit": "env-steps/s", "ms_per_step": t / K * 1e3,
+        "trajectory": f"steps {Wm}..{Wm + K - 1} after reset()",
+        "state_equal_to_restated_driver": not differ, "differing": differ}), flush=True)
+
+
+def stock_leg(args):
+    """The stock package's line for the reference arm (None when baseline/_ref is not installed)."""
+    if not os.path.exists(os.path.join(REF_PKG, "minecu", "__init__.py")):
+        return {"unavailable": "baseline/_ref is not installed"}
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--stock-leg", "--steps", str(args.steps),
+                        "--warmup", str(args.warmup)], capture_output=True, text=True, timeout=900)
+    for ln in r.stdout.splitlines():
+        if ln.startswith("STOCK "):
+            return json.loads(ln[6:])
+    return {"unavailable": f"stock-package leg failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"}
+
+
 def run_reference(args):
     """The reference's own CUDA build (oracle/_ref/libminecu_ref.so, its
     src/kernels.cu compiled unmodified) driven in its MineEnv.step order, on
@@ -931,6 +1007,9 @@ def run_reference(args):
     }
     if modes:
         line["modes"] = modes
+    if args.workload == "peak" and not args.shape:
+        # the same window through the stock package, as a cross-check of this arm's driver
+        line["stock_package"] = stock_leg(args)
     if args.workload == "peak" and not args.shape and not args.no_legs:
         del env
         legs = reference_legs(args, dev, W)
@@ -1143,10 +1222,13 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="ragged: keep the default launch configuration")
     ap.add_argument("--no-legs", action="store_true",
                     help="peak: skip the late-window, render, ragged and serve legs of the default run")
+    ap.add_argument("--stock-leg", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.stock_leg:
+        run_stock_leg(args)
+    elif args.impl == "reference":
         if args.workload == "serve":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no env server; the "
                               "one-job-at-a-time loop is the serve line's plain_one_job_at_a_time arm"}))
