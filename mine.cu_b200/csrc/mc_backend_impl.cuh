@@ -1907,22 +1907,31 @@ __host__ __device__ __forceinline__ bool up_scan_shape(int wx, int wy, int wz) {
 // lanes sweep every G-th layer, so per row a lane only ORs the row's solid
 // z mask into its column's union and notes the highest layers with a solid
 // voxel at z >= vz and at z <= vz; the column's x side and the z extremes
-// are settled once, after the sweep.
+// are settled once, after the sweep.  With nw > 1 warps sharing the scan,
+// warp w of them sweeps the layers of groups w*G .. w*G+G-1 of nw*G, and
+// the result is the warp's part of the bounds (combined by team_up_bounds).
 template <typename M>
-__device__ __forceinline__ UpBounds staged_up_bounds_t(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
-                                                       int vz, int lane) {
-    constexpr int kBits = 8 * sizeof(M);
+struct UpPart {
+    int xa0, xa1, xa2, xa3;  // x extremes of q0 (x-, z-), q1 (x+, z-), q2 (x-, z+), q3 (x+, z+)
+    int ya0, ya1, ya2, ya3;  // highest layer + 1
+    M mp, mm;                // solid z masks of the x >= vx / x <= vx columns
+};
+
+template <typename M>
+__device__ __forceinline__ UpPart<M> staged_up_part(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
+                                                    int vz, int lane, int w = 0, int nw = 1) {
     const int cpr = wz >> 4;                              // 16-byte chunks per row
+    constexpr int kBits = 8 * sizeof(M);
     const M zpm = ~M(0) << vz;                            // z >= vz
     const M zmm = (vz + 1 < kBits) ? ((M(1) << (vz + 1)) - 1) : ~M(0);  // z <= vz
     const int G = wx <= 32 ? 32 / wx : 1, g = wx <= 32 ? lane / wx : 0;
-    int xa0 = 255, xa1 = 0, xa2 = 255, xa3 = 0;  // x extremes of q0 (x-, z-), q1 (x+, z-), q2 (x-, z+), q3 (x+, z+)
-    int ya0 = 0, ya1 = 0, ya2 = 0, ya3 = 0;      // highest layer + 1
-    M mp = 0, mm = 0;                            // solid z masks of the x >= vx / x <= vx columns
+    int xa0 = 255, xa1 = 0, xa2 = 255, xa3 = 0;
+    int ya0 = 0, ya1 = 0, ya2 = 0, ya3 = 0;
+    M mp = 0, mm = 0;
     for (int x = wx <= 32 ? lane - g * wx : lane; g < G && x < wx; x += 32) {
         M mu = 0;
         int yp = 0, ym = 0;  // highest layer + 1 with a solid voxel at z >= vz / z <= vz
-        for (int y = vy + g; y < wy; y += G) {
+        for (int y = vy + w * G + g; y < wy; y += G * nw) {
             const int r = y * wx + x;
             const uint4* row = reinterpret_cast<const uint4*>(world + r * wz);
             M m = 0;
@@ -1952,25 +1961,41 @@ __device__ __forceinline__ UpBounds staged_up_bounds_t(const int8_t* world, int 
             return M(__reduce_or_sync(F, (unsigned)v)) | (M(__reduce_or_sync(F, (unsigned)(v >> 16 >> 16))) << 16 << 16);
         return M(__reduce_or_sync(F, (unsigned)v));
     };
+    UpPart<M> r;
+    r.mp = or_all(mp);
+    r.mm = or_all(mm);
+    r.xa0 = __reduce_min_sync(F, xa0);
+    r.xa1 = __reduce_max_sync(F, xa1);
+    r.xa2 = __reduce_min_sync(F, xa2);
+    r.xa3 = __reduce_max_sync(F, xa3);
+    r.ya0 = __reduce_max_sync(F, ya0);
+    r.ya1 = __reduce_max_sync(F, ya1);
+    r.ya2 = __reduce_max_sync(F, ya2);
+    r.ya3 = __reduce_max_sync(F, ya3);
+    return r;
+}
+
+// The bounds from the (combined) parts.  z extremes: over a side's solid
+// voxels the largest z is the z >= vz quadrant's extreme whenever that
+// quadrant holds any (else its y byte is 0 and the value is not used), the
+// smallest z likewise.
+template <typename M>
+__device__ __forceinline__ UpBounds up_bounds_of(const UpPart<M>& r) {
+    constexpr int kBits = 8 * sizeof(M);
     auto hi = [](M v) { return kBits - 1 - (sizeof(M) == 8 ? __clzll((long long)v) : __clz((int)v)); };
     auto lo = [](M v) { return (sizeof(M) == 8 ? __ffsll((long long)v) : __ffs((int)v)) - 1; };
-    mp = or_all(mp);
-    mm = or_all(mm);
-    // z extremes: over a side's solid voxels the largest z is the z >= vz quadrant's extreme whenever that
-    // quadrant holds any (else its y byte is 0 and the value is not used), the smallest z likewise
     UpBounds b;
-    b.x = (unsigned)__reduce_min_sync(F, xa0) | ((unsigned)__reduce_max_sync(F, xa1) << 8) |
-          ((unsigned)__reduce_min_sync(F, xa2) << 16) | ((unsigned)__reduce_max_sync(F, xa3) << 24);
-    b.z = ((unsigned)lo(mm) & 255u) | (((unsigned)lo(mp) & 255u) << 8) | (((unsigned)hi(mm) & 255u) << 16) |
-          (((unsigned)hi(mp) & 255u) << 24);
-    b.y = (unsigned)__reduce_max_sync(F, ya0) | ((unsigned)__reduce_max_sync(F, ya1) << 8) |
-          ((unsigned)__reduce_max_sync(F, ya2) << 16) | ((unsigned)__reduce_max_sync(F, ya3) << 24);
+    b.x = (unsigned)r.xa0 | ((unsigned)r.xa1 << 8) | ((unsigned)r.xa2 << 16) | ((unsigned)r.xa3 << 24);
+    b.z = ((unsigned)lo(r.mm) & 255u) | (((unsigned)lo(r.mp) & 255u) << 8) | (((unsigned)hi(r.mm) & 255u) << 16) |
+          (((unsigned)hi(r.mp) & 255u) << 24);
+    b.y = (unsigned)r.ya0 | ((unsigned)r.ya1 << 8) | ((unsigned)r.ya2 << 16) | ((unsigned)r.ya3 << 24);
     return b;
 }
+
 __device__ __forceinline__ UpBounds staged_up_bounds(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
                                                      int vz, int lane) {
-    return wz > 32 ? staged_up_bounds_t<unsigned long long>(world, wx, wy, wz, vx, vy, vz, lane)
-                   : staged_up_bounds_t<uint32_t>(world, wx, wy, wz, vx, vy, vz, lane);
+    return wz > 32 ? up_bounds_of(staged_up_part<unsigned long long>(world, wx, wy, wz, vx, vy, vz, lane))
+                   : up_bounds_of(staged_up_part<uint32_t>(world, wx, wy, wz, vx, vy, vz, lane));
 }
 
 // ---------------------------------------------------------------------------
@@ -2126,16 +2151,18 @@ __device__ __forceinline__ void build_fast_start(int4* sstart, int kind, const D
 }
 
 // Per-env facts of a render (EnvRender::bits).
-enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16 };
+// MC_ER_TSCAN: the up bounds are scanned by the whole team after its barrier.
+enum { MC_ER_DONE = 1, MC_ER_BURIED = 2, MC_ER_INSIDE = 4, MC_ER_SKIP = 8, MC_ER_STAGED = 16, MC_ER_TSCAN = 32 };
 
 // The rest of a per-warp launch for a warp whose bulk copy timed out
-// (defined after render_env): env e, already stepped, and every env the
-// warp claims after it, rendered from the worlds in global memory.  Called
-// after the main loop and out of line, so the staged path keeps its
+// (defined after render_env): env e, already stepped, then `claimed` (the
+// env a depth-2 warp has already claimed, or -1 for none), then every env
+// the warp claims after them, rendered from the worlds in global memory.
+// Called after the main loop and out of line, so the staged path keeps its
 // registers.  Returns whether any of those envs was done.
 template <int FAM, bool F32>
-__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long total_warps,
-                                                      int tile_w, int lane, FusedCtx cx);
+__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long claimed,
+                                                      long long total_warps, int tile_w, int lane, FusedCtx cx);
 
 #ifndef MC_FUSED_MIN_BLOCKS
 #define MC_FUSED_MIN_BLOCKS 4
@@ -2522,7 +2549,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         cx.s_sky8 = s_sky8;
         cx.stage = stage;
         cx.rcp_vd = rcp_vd;
-        any_done |= fused_finish_from_global<FAM, F32>(p, e, total_warps, tile_w, lane, cx);
+        any_done |= fused_finish_from_global<FAM, F32>(p, e, prefetch ? ahead : -1, total_warps, tile_w, lane, cx);
         // the timed-out copy may still be in flight: let it land (bounded, with
         // the default budget) before this warp's part of shared memory can be released
         if (pending) mbar_wait(mbar_a, pending_phase);
@@ -2572,12 +2599,17 @@ struct EnvRender {
     UpBounds ub;   // bounds of the rays going up (up_none(ytop) unless measured)
 };
 
+// Whether the eye's voxel lies in the box.
+__device__ __forceinline__ bool eye_in_box(const Cam& c, int wx, int wy, int wz) {
+    const int ex = (int)floorf(c.eye_x), ey = (int)floorf(c.eye_y), ez = (int)floorf(c.eye_z);
+    return (unsigned)ex < (unsigned)wx && (unsigned)ey < (unsigned)wy && (unsigned)ez < (unsigned)wz;
+}
+
 // Measure a staged world for the rays going up: per quadrant of the eye's
 // column when the eye's voxel lies in the box, else the top layer only.
 __device__ __forceinline__ void measure_staged(EnvRender& r, const int8_t* world, int wx, int wy, int wz, int lane) {
     const int ex = (int)floorf(r.c.eye_x), ey = (int)floorf(r.c.eye_y), ez = (int)floorf(r.c.eye_z);
-    if ((unsigned)ex < (unsigned)wx && (unsigned)ey < (unsigned)wy && (unsigned)ez < (unsigned)wz &&
-        up_scan_shape(wx, wy, wz)) {
+    if (eye_in_box(r.c, wx, wy, wz) && up_scan_shape(wx, wy, wz)) {
         r.ub = staged_up_bounds(world, wx, wy, wz, ex, ey, ez, lane);
         r.ytop = up_top(r.ub);
     } else {
@@ -2587,13 +2619,72 @@ __device__ __forceinline__ void measure_staged(EnvRender& r, const int8_t* world
 }
 
 
+// Barrier of one team (named barrier `bar`, nthreads threads).
+__device__ __forceinline__ void team_sync(int bar, int nthreads) {
+    if (nthreads == 32)
+        __syncwarp();
+    else
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+}
+
 struct TeamShared {
     unsigned unit[2];  // claimed units, alternating slots
     int band_ctr;      // next row band of the cooperative env
     int pad;
     EnvRender r;       // the cooperative env
+    // the cooperative env's up bounds, combined over the team's warps (UpPart)
+    int uxa[4], uya[4];
+    unsigned long long ump, umm;
 };
 static_assert(sizeof(TeamShared) <= MC_TEAM_HEAD_BYTES, "team head");
+
+// Reset the team's up-bound words (the stepping warp's lane 0, before the
+// barrier that publishes the env).
+__device__ __forceinline__ void team_up_reset(TeamShared* ts) {
+    ts->uxa[0] = 255; ts->uxa[1] = 0; ts->uxa[2] = 255; ts->uxa[3] = 0;
+    ts->uya[0] = ts->uya[1] = ts->uya[2] = ts->uya[3] = 0;
+    ts->ump = ts->umm = 0ull;
+}
+
+// The up bounds of a cooperative env, scanned by all nw warps of its team
+// (warp w sweeps its share of the layers, staged_up_part) and combined in
+// the team's shared words with shared-memory atomics, so every warp holds
+// the same bounds after the team barrier.  Called by every warp of the team.
+template <typename M>
+__device__ __forceinline__ UpBounds team_up_bounds_t(const int8_t* world, int wx, int wy, int wz, int vx, int vy,
+                                                     int vz, int lane, int w, int nw, TeamShared* ts, int bar) {
+    const UpPart<M> r = staged_up_part<M>(world, wx, wy, wz, vx, vy, vz, lane, w, nw);
+    if (lane == 0) {
+        atomicMin(&ts->uxa[0], r.xa0);
+        atomicMax(&ts->uxa[1], r.xa1);
+        atomicMin(&ts->uxa[2], r.xa2);
+        atomicMax(&ts->uxa[3], r.xa3);
+        atomicMax(&ts->uya[0], r.ya0);
+        atomicMax(&ts->uya[1], r.ya1);
+        atomicMax(&ts->uya[2], r.ya2);
+        atomicMax(&ts->uya[3], r.ya3);
+        atomicOr(&ts->ump, (unsigned long long)r.mp);
+        atomicOr(&ts->umm, (unsigned long long)r.mm);
+    }
+    team_sync(bar, nw * 32);
+    UpPart<M> t;
+    t.xa0 = ts->uxa[0];
+    t.xa1 = ts->uxa[1];
+    t.xa2 = ts->uxa[2];
+    t.xa3 = ts->uxa[3];
+    t.ya0 = ts->uya[0];
+    t.ya1 = ts->uya[1];
+    t.ya2 = ts->uya[2];
+    t.ya3 = ts->uya[3];
+    t.mp = (M)ts->ump;
+    t.mm = (M)ts->umm;
+    return up_bounds_of(t);
+}
+__device__ __forceinline__ UpBounds team_up_bounds(const int8_t* world, int wx, int wy, int wz, int vx, int vy, int vz,
+                                                   int lane, int w, int nw, TeamShared* ts, int bar) {
+    return wz > 32 ? team_up_bounds_t<unsigned long long>(world, wx, wy, wz, vx, vy, vz, lane, w, nw, ts, bar)
+                   : team_up_bounds_t<uint32_t>(world, wx, wy, wz, vx, vy, vz, lane, w, nw, ts, bar);
+}
 
 // Decode, episode rule, physics, interaction, reset, counters and camera of
 // env e, run by one whole warp: every lane computes the same values, lane 0
@@ -2865,8 +2956,8 @@ __device__ __forceinline__ void render_env(const mc_kp& p, long long e, const En
 }
 
 template <int FAM, bool F32>
-__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long total_warps,
-                                                      int tile_w, int lane, FusedCtx cx) {
+__device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long e, long long claimed,
+                                                      long long total_warps, int tile_w, int lane, FusedCtx cx) {
     const long long wxyz = (long long)p.wx * p.wy * p.wz;
     if (e < p.B) {
         // env e was stepped and found not buried: its camera, as stored by the
@@ -2896,7 +2987,8 @@ __device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long 
         r.ytop = p.wy - 1;
         r.ub = up_none(r.ytop);
         render_env<FAM, F32, VoxGlobal, false>(p, e, r, cx, VoxGlobal{p.voxels + e * wxyz}, tile_w, lane, nullptr);
-        e = next_env(p, e, total_warps, lane);
+        // a depth-2 warp's next env is the one it claimed already
+        e = claimed >= 0 ? claimed : next_env(p, e, total_warps, lane);
     }
     bool any_done = false;
     const ActionSrc act{p.actions, p.buttons, p.look};
@@ -2928,13 +3020,6 @@ __device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, in
     const bool ok = mbar_wait(mbar_a, phase, polls);
     phase ^= 1u;
     return ok;
-}
-
-__device__ __forceinline__ void team_sync(int bar, int nthreads) {
-    if (nthreads == 32)
-        __syncwarp();
-    else
-        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
 }
 
 #ifndef MC_TEAM_MIN_BLOCKS
@@ -3033,7 +3118,10 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                     if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
                         world[r.mod_idx] = (int8_t)r.mod_val;
                     __syncwarp();
-                    measure_staged(r, world, p.wx, p.wy, p.wz, lane);
+                    if (coop && TWN > 1 && eye_in_box(r.c, p.wx, p.wy, p.wz) && up_scan_shape(p.wx, p.wy, p.wz))
+                        r.bits |= MC_ER_TSCAN;  // the whole team scans, after the barrier
+                    else
+                        measure_staged(r, world, p.wx, p.wy, p.wz, lane);
                 } else {
                     if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
                     warp_no_stage = true;  // the copy may still land: render from global memory from now on
@@ -3045,6 +3133,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                 r.bits |= staged ? MC_ER_STAGED : 0;
                 ts->r = r;
                 ts->band_ctr = 0;
+                if (r.bits & MC_ER_TSCAN) team_up_reset(ts);
             }
             __syncwarp();
         }
@@ -3052,6 +3141,11 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
             team_sync(bar, nthr);
             r = ts->r;
             staged = (r.bits & MC_ER_STAGED) != 0;
+            if (r.bits & MC_ER_TSCAN) {  // team-uniform
+                r.ub = team_up_bounds(world, p.wx, p.wy, p.wz, (int)floorf(r.c.eye_x), (int)floorf(r.c.eye_y),
+                                      (int)floorf(r.c.eye_z), lane, wt, TWN, ts, bar);
+                r.ytop = up_top(r.ub);
+            }
         }
         if (coop || stepper) {
             if (r.bits & MC_ER_BURIED)

@@ -120,7 +120,7 @@ enum { MC_COLOUR_TABLE_BYTES = 224 };  // shared colour tables of the fused kern
 // the common-case render loop's tables (colour x shade: 13 x 4 float4; packed
 // flat colours: 13 uint32 padded to 64 bytes), after the colour tables
 enum { MC_FAST_TABLE_BYTES = 13 * 4 * 16 + 64 };
-enum { MC_TEAM_HEAD_BYTES = 128 };     // per-team shared words ahead of the team's world buffer
+enum { MC_TEAM_HEAD_BYTES = 256 };     // per-team shared words ahead of the team's world buffer
 enum { MC_ENV_STASH_BYTES = 96 };      // one env's render constants, kept in shared memory (depth 2)
 struct mc_ragged_kp {
     mc_kp groups[MC_MAX_GROUPS];    // the groups' parameter blocks (kernel parameter space)

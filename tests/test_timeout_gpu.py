@@ -97,3 +97,33 @@ def test_copy_timeout_in_a_ragged_launch(cuda):
         batch.check_error()
     for e in sb:
         e.check_error()
+
+
+def test_copy_timeout_depth2_keeps_claimed_envs(cuda):
+    """Staging depth 2 with more envs than the grid has warps: every warp
+    claims its next env one ahead, so each warp whose wait runs out holds a
+    claimed env that it must still step and render from global memory.  The
+    result equals the same envs stepped with the default budget (no
+    timeouts), bit for bit, at every step."""
+    from mc_harness import GpuEnv
+    L = capi.lib()
+    B = 9600  # above 148 SMs x 4 CTAs x 8 warps: two or more envs per warp
+    envs = []
+    for limit in (0, -1):
+        g = GpuEnv(cuda, B, numerics="ieee", obs_dtype="uint8", debug=False)
+        g.set_fused(2, 8, 4, 4, 1, 0)
+        capi.check(L.mc_env_set_wait_limit(g.h, limit), "set_wait_limit")
+        g.reset()
+        envs.append(g)
+    timed_out, normal = envs
+    for s in range(12):
+        _, btn, look = actions_for(B, s, 31, break_half=True)
+        timed_out.step(btn, look, capi.FORM_FUSED)
+        normal.step(btn, look, capi.FORM_FUSED)
+        d = diff_report(timed_out.state(), normal.state())
+        assert not d, f"step {s}: {d}"
+    assert L.mc_env_check_error(timed_out.h, None) == capi.MC_ERR_KERNEL
+    assert "timed out" in capi.last_error()
+    normal.check_error()
+    for g in envs:
+        g.close()
