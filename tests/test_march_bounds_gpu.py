@@ -4,11 +4,11 @@ solid voxels (the per-env scan of the staged world, staged_up_bounds).
 Random scenes: sparse blocks of every kind above a solid ground, eyes
 anywhere in the open (above and below the blocks, next to the box's faces),
 every yaw and a wide range of pitches, stepped through both fused kernels
-(per-warp and cooperative team, staging depth 1 and 2) without debug
-outputs, so that the common-case loop runs.  World shapes cover rows of 16
-and 32 bytes (32-bit masks), 48 bytes (64-bit masks) and 20 bytes (no scan:
-the top layer only).  Compared with the CPU oracle bit for bit: every state
-field and observation byte.
+(per-warp, and cooperative teams of 2, 4 and 8 warps that share the scan;
+staging depth 1 and 2) without debug outputs, so that the common-case loop
+runs.  World shapes cover rows of 16 and 32 bytes (32-bit masks), 48 bytes
+(64-bit masks) and 20 bytes (no scan: the top layer only).  Compared with
+the CPU oracle bit for bit: every state field and observation byte.
 """
 import zlib
 
@@ -33,6 +33,9 @@ SHAPES = {
 CFGS = {
     "per_warp": (1, 8, 4, 4, 1, 0),
     "team": (1, 8, 3, 8, 4, 1),
+    # the team's warps share the scan (team_up_bounds): teams of 2 and 8 too
+    "team2": (1, 8, 3, 8, 2, 1),
+    "team8": (1, 8, 2, 16, 8, 1),
     "team_depth2": (2, 8, 2, 8, 4, 1),
     "per_warp_depth2": (2, 8, 4, 4, 1, 0),
 }
