@@ -3004,9 +3004,8 @@ __device__ __noinline__ bool fused_finish_from_global(const mc_kp& p, long long 
     return any_done;
 }
 
-// Bulk copy of one world into shared memory, waited for with a bound.
-__device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, int8_t* dst, const int8_t* src,
-                                            int bytes, int lane, int polls) {
+// Start the bulk copy of one world into shared memory (lane 0 issues it).
+__device__ __forceinline__ void issue_world_copy(uint32_t mbar_a, int8_t* dst, const int8_t* src, int bytes, int lane) {
     if (lane == 0) {
         // generic-proxy reads of the previous world must precede the copy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -3017,6 +3016,12 @@ __device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, in
             "l"(src), "r"(bytes), "r"(mbar_a)
             : "memory");
     }
+}
+
+// Bulk copy of one world into shared memory, waited for with a bound.
+__device__ __forceinline__ bool stage_world(uint32_t mbar_a, uint32_t& phase, int8_t* dst, const int8_t* src,
+                                            int bytes, int lane, int polls) {
+    issue_world_copy(mbar_a, dst, src, bytes, lane);
     const bool ok = mbar_wait(mbar_a, phase, polls);
     phase ^= 1u;
     return ok;
@@ -3094,6 +3099,19 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
             const long long s0 = rk.start[g];
             const ActionSrc act{rk.actions ? rk.actions + s0 : nullptr, rk.actions ? nullptr : rk.buttons + 8 * s0,
                                 rk.actions ? nullptr : rk.look + 2 * s0};
+            // the world's bulk copy starts before the agent step, which it
+            // overlaps (the voxel the interaction changes is patched in after it
+            // lands); a buried env's copy is waited for and not used
+            bool copying = ((rk.stage_mask >> g) & 1) && !warp_no_stage;
+#if MC_CHECK_BOUNDS
+            if (copying) {
+                const SmemRange dyn = dyn_smem_range();
+                const long long off = (long long)smem_u32(world) - dyn.lo;
+                if (!in_bounds(off, dyn.span, MC_SITE_STAGE) || !in_bounds(off + wxyz - 1, dyn.span, MC_SITE_STAGE))
+                    copying = false;  // no copy issued: render from global memory
+            }
+#endif
+            if (copying) issue_world_copy(cx.mbar_a, world, gw, wxyz, lane);
             r = agent_step<FAM>(p, act, e, lane);
             if (lane == 0) {
                 if (r.bits & MC_ER_DONE) done_groups |= 1u << g;
@@ -3102,18 +3120,17 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                     rk.dones_cat[rk.start[g] + e] = (uint8_t)(r.bits & MC_ER_DONE);
                 }
             }
-            staged = ((rk.stage_mask >> g) & 1) && !(r.bits & MC_ER_BURIED) && !warp_no_stage;
-#if MC_CHECK_BOUNDS
-            if (staged) {
-                const SmemRange dyn = dyn_smem_range();
-                const long long off = (long long)smem_u32(world) - dyn.lo;
-                if (!in_bounds(off, dyn.span, MC_SITE_STAGE) || !in_bounds(off + wxyz - 1, dyn.span, MC_SITE_STAGE))
-                    staged = false;  // no copy issued: render from global memory
-            }
-#endif
-            if (staged) {
+            staged = copying && !(r.bits & MC_ER_BURIED);
+            if (copying) {
                 const uint32_t ph = phase;
-                if (stage_world(cx.mbar_a, phase, world, gw, wxyz, lane, p.wait_polls)) {
+                const bool landed = mbar_wait(cx.mbar_a, phase, p.wait_polls);
+                phase ^= 1u;
+                if (!landed) {
+                    if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
+                    warp_no_stage = true;  // the copy may still land: render from global memory from now on
+                    pending_phase = ph;
+                    staged = false;
+                } else if (staged) {
                     // the interaction may have written after the copy read the byte
                     if (lane == 0 && r.mod_idx >= 0 && in_bounds(r.mod_idx, wxyz, MC_SITE_PATCH))
                         world[r.mod_idx] = (int8_t)r.mod_val;
@@ -3122,11 +3139,6 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
                         r.bits |= MC_ER_TSCAN;  // the whole team scans, after the barrier
                     else
                         measure_staged(r, world, p.wx, p.wy, p.wz, lane);
-                } else {
-                    if (lane == 0) atomicExch(&p.flags[MC_FLAG_ERROR], MC_KERR_TMA_TIMEOUT);
-                    warp_no_stage = true;  // the copy may still land: render from global memory from now on
-                    pending_phase = ph;
-                    staged = false;
                 }
             }
             if (coop && lane == 0) {
