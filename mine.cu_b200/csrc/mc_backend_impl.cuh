@@ -2282,6 +2282,10 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                 p.do_reset[e] = done ? 1 : 0;
             }
             p.rewards[e] = reward;
+            if (p.res_rewards) {
+                p.res_rewards[e] = reward;
+                p.res_dones[e] = done ? 1 : 0;
+            }
             p.cameras[e * 5 + 0] = a.x;
             p.cameras[e * 5 + 1] = a.y;
             p.cameras[e * 5 + 2] = a.z;
@@ -2713,6 +2717,10 @@ __device__ __forceinline__ EnvRender agent_step(const mc_kp& p, const ActionSrc&
             p.do_reset[e] = done ? 1 : 0;
         }
         p.rewards[e] = reward;
+        if (p.res_rewards) {
+            p.res_rewards[e] = reward;
+            p.res_dones[e] = done ? 1 : 0;
+        }
         p.cameras[e * 5 + 0] = a.x;
         p.cameras[e * 5 + 1] = a.y;
         p.cameras[e * 5 + 2] = a.z;

@@ -102,6 +102,10 @@ struct mc_kp {
     float* s_speed;
     int32_t* flags;               // MC_FLAG_* words
     const int8_t* world_template; // one generated world (wx*wy*wz bytes)
+    // optional (per-warp fused kernel only): every env's reward and done also
+    // written here, in env order (the host-buffer step's read-back buffer)
+    float* res_rewards;
+    uint8_t* res_dones;
 };
 
 // Launch shape of the fused step kernel (chosen by the autotuner).

@@ -883,8 +883,11 @@ extern "C" int mc_env_reset(mc_env* e, const uint8_t* mask, void* stream) {
     return render_obs(e, s);
 }
 
+// res_rewards / res_dones: where the per-warp fused kernel also writes every
+// env's reward and done (the host-buffer step's read-back buffer); the other
+// launch forms ignore them.
 static int do_step(mc_env* e, const int8_t* buttons, const float* look, const uint8_t* actions, int form,
-                   cudaStream_t s) {
+                   cudaStream_t s, float* res_rewards = nullptr, uint8_t* res_dones = nullptr) {
     if (e->cfg.batch_size == 0) return MC_OK;
     mc_kp k = e->kp;
     k.buttons = buttons;
@@ -911,6 +914,8 @@ static int do_step(mc_env* e, const int8_t* buttons, const float* look, const ui
         rc = backend_rc(e->be->step_team(&rk, k.family, k.obs_f32, f.warps_per_cta, f.ctas_per_sm, e->num_sms, s),
                         "step_team");
     } else if (form == MC_FORM_FUSED) {
+        k.res_rewards = res_rewards;
+        k.res_dones = res_dones;
         rc = backend_rc(e->be->step_fused(&k, &e->fcfg, e->num_sms, s), "step_fused");
     } else {
         return fail(MC_ERR_INVALID, "unknown form %d", form);
@@ -1013,14 +1018,21 @@ extern "C" int mc_env_step_host(mc_env* e, const uint8_t* host_actions, float* h
     const int i = (int)(h->calls & 1);
     rc = hostio_upload(h, i, host_actions, B, s);
     if (rc) return rc;
-    rc = do_step(e, nullptr, nullptr, h->d_act[i], form, s);
+    // results go into this call's buffer once the read-back two calls back
+    // is done with it; the per-warp fused kernel writes them there itself,
+    // the other forms through a copy kernel after the step
+    MC_CK(cudaStreamWaitEvent(s, h->res_free[i], 0));
+    const bool direct = form == MC_FORM_FUSED && !team_mode(e->fcfg);
+    float* res_rew = reinterpret_cast<float*>(h->d_res[i]);
+    uint8_t* res_done = h->d_res[i] + 4 * B;
+    rc = do_step(e, nullptr, nullptr, h->d_act[i], form, s, direct ? res_rew : nullptr, direct ? res_done : nullptr);
     if (rc) return rc;
     MC_CK(cudaEventRecord(h->act_free[i], s));
-    // results into this call's buffer once the read-back two calls back is done with it
-    MC_CK(cudaStreamWaitEvent(s, h->res_free[i], 0));
-    const int grid = (int)std::min<long long>((B + 255) / 256, (long long)e->num_sms * 4);
-    k_results_snapshot<<<grid, 256, 0, s>>>(e->st.rewards, e->st.do_reset, B, h->d_res[i]);
-    MC_CK(cudaGetLastError());
+    if (!direct) {
+        const int grid = (int)std::min<long long>((B + 255) / 256, (long long)e->num_sms * 4);
+        k_results_snapshot<<<grid, 256, 0, s>>>(e->st.rewards, e->st.do_reset, B, h->d_res[i]);
+        MC_CK(cudaGetLastError());
+    }
     return hostio_readback(h, i, host_rewards, host_dones, B, s);
 }
 

@@ -62,6 +62,51 @@ def test_step_host_matches_step(cuda, form, shape):
         assert torch.equal(a, b), k
 
 
+@pytest.mark.parametrize("launch,wait0", [((0, 8, 4, 4, 1, 0), False), ((2, 8, 4, 4, 1, 0), False),
+                                          ((1, 8, 4, 4, 1, 0), True), ((2, 8, 4, 4, 1, 0), True)],
+                         ids=["depth0", "depth2", "depth1_timeouts", "depth2_timeouts"])
+def test_step_host_per_warp_launches(cuda, launch, wait0):
+    """The per-warp fused kernel writes every env's reward and done into the
+    read-back buffer itself (no copy kernel): at staging depth 0 and 2, and
+    with every bulk-copy wait made to run out, where the global-memory path
+    steps the envs.  The host results equal step(actions)'s."""
+    import torch
+    from minecu import _C
+    shape = dict(batch_size=300, world_size=16, render_width=32, render_height=32, episode_length=7,
+                 obs_dtype="uint8")
+    ref, host = _pair(cuda, "fused", **shape)
+    host.set_launch_config(*launch)
+    if wait0:
+        host.set_wait_limit(0)
+    B, K = shape["batch_size"], 15
+    acts = torch.empty((K, B), dtype=torch.uint8, device=cuda)
+    _C.philox_actions(acts, 0, 0, 13, True)
+    h_acts = acts.cpu().pin_memory()
+    h_rew = torch.zeros((K, B), dtype=torch.float32).pin_memory()
+    h_done = torch.zeros((K, B), dtype=torch.bool).pin_memory()
+    want_rew, want_done = [], []
+    for s in range(K):
+        _, r, d = ref.step(acts[s])
+        want_rew.append(r.clone())
+        want_done.append(d.clone())
+        host.step_host(h_acts[s], h_rew[s], h_done[s])
+    host.join_host()
+    torch.cuda.synchronize()
+    assert torch.equal(h_rew.view(torch.int32), torch.stack(want_rew).cpu().view(torch.int32))
+    assert torch.equal(h_done, torch.stack(want_done).cpu().to(torch.bool))
+    assert bool(torch.stack(want_done).any()) and bool((torch.stack(want_rew) != 0).any())
+    if wait0:
+        with pytest.raises(RuntimeError, match="timed out"):
+            host.check_error()
+    else:
+        host.check_error()
+    for k in KEYS:
+        a, b = getattr(ref, k), getattr(host, k)
+        if a.dtype == torch.float32:
+            a, b = a.view(torch.int32), b.view(torch.int32)
+        assert torch.equal(a, b), k
+
+
 def test_step_host_rejects_device_and_pageable_buffers(cuda):
     import torch
     from minecu import MineEnv
