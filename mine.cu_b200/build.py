@@ -119,7 +119,7 @@ def build_torch_ext(verbose: bool = False) -> str:
         verbose=verbose,
     )
     built = os.path.join(bdir, "_C.so")
-    shutil.copy2(built, target + ".tmp")
+    shutil.copy(built, target + ".tmp")  # a fresh mtime: the next build sees it up to date
     os.replace(target + ".tmp", target)
     return target
 
