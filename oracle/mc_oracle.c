@@ -42,6 +42,8 @@ static const uint8_t SKY8[3] = {135, 206, 235};
 float orc_sinf(float x) { return mc_ieee_sinf(x); }
 float orc_cosf(float x) { return mc_ieee_cosf(x); }
 float orc_tanf(float x) { return mc_ieee_tanf(x); }
+/* The Philox4x32-10 block function of the action stream, for known-answer tests. */
+void orc_philox4x32_10(uint32_t* ctr, uint32_t k0, uint32_t k1) { mc_philox4x32_10(ctr, k0, k1); }
 
 static void set_threads(int threads) {
 #ifdef _OPENMP

@@ -90,6 +90,7 @@ def lib():
         for n in ("orc_sinf", "orc_cosf", "orc_tanf"):
             getattr(L, n).restype = F
             getattr(L, n).argtypes = [F]
+        L.orc_philox4x32_10.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32]
         _lib = L
     return _lib
 
@@ -212,6 +213,14 @@ def discrete_to_buttons(actions: np.ndarray, look_delta: float):
     look = np.zeros((B, 2), np.float32)
     lib().orc_discrete_to_buttons(_p(a), B, look_delta, _p(btn), _p(look))
     return btn, look
+
+
+def philox4x32_10(ctr, key):
+    """One Philox4x32-10 block (the action stream's generator): 4 counter
+    words and 2 key words in, 4 words out."""
+    c = np.ascontiguousarray(np.array(ctr, dtype=np.uint32))
+    lib().orc_philox4x32_10(c.ctypes.data, int(key[0]), int(key[1]))
+    return tuple(int(v) for v in c)
 
 
 def sinf(x: float) -> float:
