@@ -2225,24 +2225,26 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     }
     __syncthreads();
     uint32_t phase = 0;
-    bool any_done = false;
     bool no_stage = false;        // a copy timed out: this warp renders from global memory from now on
     bool pending = false;         // ... and that copy may still be in flight
     uint32_t pending_phase = 0;   // its phase, waited for before the warp leaves
-    const float rcp_vd = N::rcp_of(p.vd);
+    // The kernel runs at its 64-register budget: values that would stay live
+    // across the env loop are recomputed where they are used (1 / vd, the
+    // env sizes) or not kept at all (the any-done flag goes straight to the
+    // flag word), and env indices are 32-bit (fewer spills, measured faster).
 
-    const long long obs_env_bytes = (long long)HW * 3 * (F32 ? 4 : 1);
-    const long long total_warps = (long long)gridDim.x * nwarps;
-    const long long first = p.sched_dynamic ? next_env(p, 0, total_warps, lane) : (long long)blockIdx.x * nwarps + warp;
-    long long e = first;
+    const int obs_env_bytes = HW * 3 * (F32 ? 4 : 1);
+    const int total_warps = gridDim.x * nwarps;
+    const int first = p.sched_dynamic ? (int)next_env(p, 0, total_warps, lane) : blockIdx.x * nwarps + warp;
+    int e = first;
     // staging depth 2 (prefetch): the warp claims its next env one ahead and,
     // while it steps and renders this one, prefetches that env's world (and
     // the state the step reads) into L2, so the next bulk copy reads L2
-    long long ahead = (prefetch && e < p.B) ? next_env(p, e, total_warps, lane) : p.B;
-    auto advance = [&]() -> long long {
-        if (!prefetch) return next_env(p, e, total_warps, lane);
-        const long long r = ahead;
-        ahead = r < p.B ? next_env(p, r, total_warps, lane) : r;
+    int ahead = (prefetch && e < p.B) ? (int)next_env(p, e, total_warps, lane) : p.B;
+    auto advance = [&]() -> int {
+        if (!prefetch) return (int)next_env(p, e, total_warps, lane);
+        const int r = ahead;
+        ahead = r < p.B ? (int)next_env(p, r, total_warps, lane) : r;
         return r;
     };
     for (; e < p.B; e = advance()) {
@@ -2274,7 +2276,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         int8_t mod_val;
         int mod_idx = interact_warp(gw, a, d.brk, d.place, p, lane, &reward, &mod_val);
         if (done) reset_agent(a, p);
-        any_done |= done;
+        if (done && lane == 0) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);  // rare: no per-warp accumulator
         if (lane == 0) {
             store_agent(p, e, a);
             if (!p.ext_done) {
@@ -2338,7 +2340,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                          !(FAM == MC_FAM_SHADED_FAST && ey < p.gh);
         else
             skip_first = p.max_steps > 0 && !(eye_inb && eye_blk >= 0);
-        uint8_t* oenv = (uint8_t*)p.obs + e * obs_env_bytes;
+        uint8_t* oenv = (uint8_t*)p.obs + (long long)e * obs_env_bytes;
         const bool vec_ok = ((obs_env_bytes & 15) == 0) && ((((uintptr_t)oenv) & 15) == 0);
         if (buried) {
             Hit h;
@@ -2349,8 +2351,8 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
             uint8_t bytes[12];
             if (F32 || FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                 float rgb[3];
-                shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(h, p.vd, rcp_vd,
-                                                                                                      s_rgb, s_sky, rgb);
+                shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
+                    h, p.vd, N::rcp_of(p.vd), s_rgb, s_sky, rgb);
                 if (F32) {
                     // pattern period 12 bytes
 #pragma unroll
@@ -2382,11 +2384,11 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                 fill_pattern16(oenv, (int)obs_env_bytes, make_uint4(w[0], w[1], w[2], w[3]),
                                make_uint4(w[4], w[5], w[6], w[7]), make_uint4(w[8], w[9], w[10], w[11]), lane);
             } else {
-                for (long long k = lane; k < obs_env_bytes; k += 32) oenv[k] = bytes[k % period];
+                for (int k = lane; k < obs_env_bytes; k += 32) oenv[k] = bytes[k % period];
             }
             if (p.dbg_pixel) {
                 int16_t code = dbg_code(h);
-                for (int k = lane; k < HW; k += 32) p.dbg_pixel[e * HW + k] = code;
+                for (int k = lane; k < HW; k += 32) p.dbg_pixel[(long long)e * HW + k] = code;
             }
             continue;
         }
@@ -2466,7 +2468,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                 fe.base = fk == 1 ? wb : wb + (uint32_t)(d0.vy * wxz + d0.vx * p.wz + d0.vz);
                 fe.chk = staged_range(wb, wxz, wxyz);
                 fe.vd = p.vd;
-                fe.rcp_vd = rcp_vd;
+                fe.rcp_vd = N::rcp_of(p.vd);
                 for (int row0 = 0; row0 < H; row0 += TH) {
                     uint8_t* dst = oenv + (long long)row0 * W * (3 * (F32 ? 4 : 1));
                     if (fk == 1)
@@ -2505,7 +2507,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                     if (FAM == MC_FAM_SHADED || FAM == MC_FAM_SHADED_FAST) {
                         float rgb[3];
                         shade_rgb<F32 ? MC_COL_F32 : (FAM == MC_FAM_SHADED_FAST ? MC_COL_U8FAST : MC_COL_U8)>(
-                            h, p.vd, rcp_vd, s_rgb, s_sky, rgb);
+                            h, p.vd, N::rcp_of(p.vd), s_rgb, s_sky, rgb);
                         if (F32) {
                             float* sf = reinterpret_cast<float*>(stage) + so * 3;
                             sf[0] = rgb[0]; sf[1] = rgb[1]; sf[2] = rgb[2];
@@ -2521,7 +2523,7 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
                         sb[0] = col[0]; sb[1] = col[1]; sb[2] = col[2];
                     }
                     if (p.dbg_pixel && in_bounds(py * W + px, HW, MC_SITE_DEBUG))
-                        p.dbg_pixel[e * HW + py * W + px] = dbg_code(h);
+                        p.dbg_pixel[(long long)e * HW + py * W + px] = dbg_code(h);
                 }
             }
             __syncwarp();
@@ -2552,8 +2554,9 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
         cx.s_rgb8 = s_rgb8;
         cx.s_sky8 = s_sky8;
         cx.stage = stage;
-        cx.rcp_vd = rcp_vd;
-        any_done |= fused_finish_from_global<FAM, F32>(p, e, prefetch ? ahead : -1, total_warps, tile_w, lane, cx);
+        cx.rcp_vd = N::rcp_of(p.vd);
+        if (fused_finish_from_global<FAM, F32>(p, e, prefetch ? ahead : -1, total_warps, tile_w, lane, cx) && lane == 0)
+            atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
         // the timed-out copy may still be in flight: let it land (bounded, with
         // the default budget) before this warp's part of shared memory can be released
         if (pending) mbar_wait(mbar_a, pending_phase);
@@ -2561,7 +2564,6 @@ __global__ void __launch_bounds__(256, MC_FUSED_MIN_BLOCKS) k_step_fused(const _
     // No CTA barrier here: warps leave as soon as their last env is done.
     if (lane == 0) {
         bounds_to_flags(p.flags);
-        if (any_done) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
         if (p.sched_dynamic) {
             // every claim of this warp has returned (the last one >= B); the
             // last warp to get here resets the counters for the next launch
@@ -2842,7 +2844,7 @@ __device__ __forceinline__ void fill_env(const mc_kp& p, long long e, const EnvR
     }
     if (p.dbg_pixel) {
         int16_t code = dbg_code(h);
-        for (int k = t; k < HW; k += nt) p.dbg_pixel[e * HW + k] = code;
+        for (int k = t; k < HW; k += nt) p.dbg_pixel[(long long)e * HW + k] = code;
     }
 }
 
