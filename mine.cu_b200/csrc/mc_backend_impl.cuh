@@ -3081,7 +3081,6 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     __syncthreads();
     const int bar = 1 + team, nthr = TWN * 32;
     uint32_t phase = 0;
-    unsigned done_groups = 0;
     bool warp_no_stage = false;   // a copy of this warp timed out: it renders from global memory from now on
     uint32_t pending_phase = 0;   // that copy's phase, waited for before the warp leaves
     for (int k = 0;; ++k) {
@@ -3124,7 +3123,9 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
             if (copying) issue_world_copy(cx.mbar_a, world, gw, wxyz, lane);
             r = agent_step<FAM>(p, act, e, lane);
             if (lane == 0) {
-                if (r.bits & MC_ER_DONE) done_groups |= 1u << g;
+                // rare: set as the env ends (a per-team mask of groups would
+                // stay live across the loop and spill)
+                if (r.bits & MC_ER_DONE) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);
                 if (rk.rewards_cat) {
                     rk.rewards_cat[rk.start[g] + e] = p.rewards[e];
                     rk.dones_cat[rk.start[g] + e] = (uint8_t)(r.bits & MC_ER_DONE);
@@ -3184,8 +3185,6 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team(const __g
     if (warp_no_stage) mbar_wait(cx.mbar_a, pending_phase);
     if (lane == 0) {
         for (int g = 0; g < G; ++g) bounds_to_flags(rk.groups[g].flags);
-        for (int g = 0; g < G; ++g)
-            if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);
     }
     if (claimer && rk.sched_dynamic) finish_dynamic(rk.flags, total_teams);
 }

@@ -34,8 +34,6 @@ constexpr size_t kPerEnv = 5 * sizeof(float) + 3;  // fwd, strafe, dyaw, dpitch,
 constexpr size_t kScratchBytes = kFlagBytes + ((size_t)MC_NOALLOC_MAX_ENVS * kPerEnv + 255) / 256 * 256;
 static_assert(kFlagBytes >= MC_FLAG_WORDS * sizeof(int32_t), "the flag words must fit in front of the scratch");
 static_assert(kFlagBytes % 16 == 0, "the decode arrays after the flag words stay 16-byte aligned");
-static_assert(kFlagBytes >= MC_FLAG_WORDS * sizeof(int32_t), "the flag words must fit in front of the scratch");
-static_assert(kFlagBytes % 16 == 0, "the decode arrays after the flag words stay 16-byte aligned");
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kScratchBytes];
 
