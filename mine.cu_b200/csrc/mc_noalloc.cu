@@ -14,8 +14,6 @@
 // cudaGetSymbolAddress (with that device current); make that first call
 // before any stream capture.  The address is kept for the life of the
 // process, so cudaDeviceReset on a device while the library is loaded is
-// not supported (the kept address would no longer name the array).  The address is kept for the life of the
-// process, so cudaDeviceReset on a device while the library is loaded is
 // not supported (the kept address would no longer name the array).  Every
 // call shares the one array, so calls that overlap on the GPU (different
 // streams, or different host threads on the same device) race on it.
