@@ -53,7 +53,7 @@ RENDER_METRIC = "env-steps/s at B=4096, W=32, 64x64, half break actions (fused s
 TRAFFIC = {
     "peak": (113.2e6 + 60.8e6, "k_step_fused, step 701, profiles/k_step_fused_peak_late_full.md"),
     "render": (135.3e6 + 28.4e6, "k_step_team, step 301, profiles/k_step_team_B4096_w32_r64_full.md"),
-    "ragged": (70.8e6 + 15.5e6, "k_step_team, mean of its 75 launches, profiles/k_step_team_ragged_launches.md"),
+    "ragged": (70.7e6 + 15.3e6, "k_step_team, mean of its 75 launches, profiles/k_step_team_ragged_launches.md"),
 }
 
 
