@@ -3248,7 +3248,6 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
     __syncthreads();
     const int bar = 1 + team, nthr = TWN * 32;
     uint32_t phases = 0;          // bit d: parity of depth slot d's next wait
-    unsigned done_groups = 0;
     bool warp_no_stage = false;   // a copy of this warp timed out: no more copies, render from global memory
     uint32_t pending = 0;         // bit d: a timed-out copy into slot d may still be in flight
     uint32_t pending_phases = 0;  // bit d: its parity
@@ -3284,7 +3283,7 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
                             rk.actions ? nullptr : rk.look + 2 * s0};
         EnvRender r = agent_step<FAM>(p, act, t.e, lane);
         if (lane == 0) {
-            if (r.bits & MC_ER_DONE) done_groups |= 1u << t.g;
+            if (r.bits & MC_ER_DONE) atomicOr(&p.flags[MC_FLAG_ANY_DONE], 1);  // rare: set as the env ends
             if (rk.rewards_cat) {
                 rk.rewards_cat[s0 + t.e] = p.rewards[t.e];
                 rk.dones_cat[s0 + t.e] = (uint8_t)(r.bits & MC_ER_DONE);
@@ -3383,8 +3382,6 @@ __global__ void __launch_bounds__(256, MC_TEAM_MIN_BLOCKS) k_step_team2(const __
         if ((pending >> d) & 1u) mbar_wait(mbar0 + 8 * d, (pending_phases >> d) & 1u);
     if (lane == 0) {
         for (int g = 0; g < G; ++g) bounds_to_flags(rk.groups[g].flags);
-        for (int g = 0; g < G; ++g)
-            if ((done_groups >> g) & 1) atomicOr(&rk.groups[g].flags[MC_FLAG_ANY_DONE], 1);
     }
     if (claimer && rk.sched_dynamic) finish_dynamic(rk.flags, total_teams);
 }
